@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""bench.py -- throughput of the plain GPU method on one range: sieve + Freudenthal search
+over the odd sums 5..2^21 (`ff_sieve 5 2097152`), byte-identical to the reference.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One step = the whole job for the range: the reference's full prime map (values up to
+274,877,906,959, 16 GiB) sieved on the device, then every odd sum of the range searched,
+leaving one packed record per sum in HBM. `value` is odd sums per second of that job on
+device-resident data (CUDA events on the launching stream, max over ranks); `e2e` is the
+same metric through the public call a user makes (ffb_run: sieve, search, records copied
+to the host, the text emitted in ff_seg's order), timed on the host clock.
+
+--impl reference times the reference program itself (ff_seg, compiled from the
+reference's source) on the host cores: a bounded sample of the same job (see
+reference_arm()).
+
+With N > 1 ranks (torchrun), the sums are split into cost-balanced contiguous shards, one
+per GPU; each rank sieves the map its shard needs and searches its shard, and the records
+are gathered to rank 0 over NCCL (strong scaling: the job is fixed).
+"""
+import argparse
+import ctypes
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ff-gpu_b200"))
+
+LIMIT = 2097152
+METRIC = "sums/sec byte-identical at sumLimit=2^21; served p50/p99 latency vs plain"
+UNIT = "sums/s"
+
+
+def odd_sums(lo, hi):
+    return (hi - lo) // 2 + 1 if hi >= lo else 0
+
+
+# ---------------------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------------------
+def shard_bounds(lo, hi, world, rank):
+    """Contiguous shard [a, b] of the odd sums lo..hi for `rank`, balanced by the search
+    cost, which grows about linearly with the sum (the cumulative cost ~ s^2)."""
+    import math
+    if world == 1:
+        return lo, hi
+
+    def cut(q):  # sum s with (s^2 - lo^2) / (hi^2 - lo^2) = q, made odd
+        s = int(math.sqrt(lo * lo + q * (hi * hi - lo * lo)))
+        return max(lo, min(hi, s | 1))
+    a = lo if rank == 0 else cut(rank / world)
+    b = hi if rank == world - 1 else cut((rank + 1) / world) - 2
+    return a, b
+
+
+def geometry_for(ffb, limit):
+    g, _ = ffb.geometry(5, limit)
+    return g
+
+
+def ours(args, rank, world, dist):
+    import torch
+    import ffb200 as ffb
+    lib = ffb.load()
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    g = geometry_for(ffb, LIMIT)
+    lo, hi = 5, LIMIT - 1                                  # odd sums of `ff_sieve 5 2097152`
+    a, b = shard_bounds(lo, hi, world, rank)
+    # the map this shard's probes need: the reference's map for the shard's top sum
+    gs = geometry_for(ffb, b + 1)
+    mpv = gs.maxPrimeMapValue
+    nsums = odd_sums(a, b)
+    d_map = torch.empty(((mpv + 1 + 15) >> 4) + 64, dtype=torch.uint8, device="cuda")
+    d_rec = torch.empty(max(nsums, 1), dtype=torch.int64, device="cuda")
+    stream = torch.cuda.Stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def step(ev=None):
+        if ev:
+            ev[0].record(stream)
+        assert lib.ffb_sieve_map_async(dev, mpv, d_map.data_ptr(), sp) == 0
+        if ev:
+            ev[1].record(stream)
+        assert lib.ffb_search_async(dev, d_map.data_ptr(), mpv, a, b, d_rec.data_ptr(), sp) == 0
+        if ev:
+            ev[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    assert ffb.take_errors(dev) == 0
+    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(dev)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    t0.record(stream)
+    for k in range(args.steps):
+        step(evs[k])
+    t1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    if dist:
+        dist.barrier()
+    total_ms = t0.elapsed_time(t1)
+    sieve_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in evs)
+    search_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in evs)
+    flags = ffb.take_errors(dev)
+    if flags:
+        raise RuntimeError(f"device error flags {flags:#x}")
+    # records of all shards to rank 0 (the exchange of the sharded job)
+    if dist and world > 1:
+        sizes = [odd_sums(*shard_bounds(lo, hi, world, r)) for r in range(world)]
+        buf = torch.zeros(max(sizes), dtype=torch.int64, device="cuda")
+        buf[:nsums] = d_rec[:nsums]
+        gathered = [torch.empty_like(buf) for _ in range(world)]
+        dist.all_gather(gathered, buf)
+    t = torch.tensor([total_ms, sieve_ms, search_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms, sieve_ms, search_ms = t.tolist()
+    ms_per_step = total_ms / args.steps
+    job_sums = odd_sums(lo, hi)
+    value = job_sums / (ms_per_step / 1e3)
+
+    # e2e through the public call (rank 0, the whole job on one GPU)
+    e2e = None
+    if rank == 0:
+        ctx = lib.ffb_context_create(dev)
+        p, n = ctypes.c_void_p(), ctypes.c_size_t()
+        for _ in range(max(1, args.warmup)):
+            assert lib.ffb_run(ctx, 2, 5, LIMIT, ctypes.byref(p), ctypes.byref(n)) == 0
+            lib.ffb_free(p)
+        times = []
+        text_len = 0
+        for _ in range(args.steps):
+            s = time.perf_counter()
+            assert lib.ffb_run(ctx, 2, 5, LIMIT, ctypes.byref(p), ctypes.byref(n)) == 0
+            times.append(time.perf_counter() - s)
+            text_len = n.value
+            lib.ffb_free(p)
+        lib.ffb_context_destroy(ctx)
+        e2e = {"value": job_sums / statistics.mean(times), "unit": UNIT,
+               "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8 * job_sums,
+               "text_bytes_per_step": text_len, "ms_per_step": 1e3 * statistics.mean(times)}
+
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    map_bytes = (mpv + 1 + 15) >> 4
+    # dominant kernel of the step
+    if sieve_ms >= search_ms:
+        achieved = map_bytes / (sieve_ms / 1e3) / 1e9
+        roof = {"kernel": "sieve_tiles", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "algorithmic_bytes": map_bytes, "peak_source": peak_src,
+                "note": "algorithmic bytes = bitmap bytes written once"}
+    else:
+        # search: random 32-byte sector probes of the map; algorithmic bytes per step =
+        # 32 B x the HBM-bound probes (2^k + o*b - 2 of the splits that pass the cheap test)
+        probes = SEARCH_DRAM_PROBES.get(LIMIT)
+        achieved = (32 * probes / (search_ms / 1e3) / 1e9) if probes else None
+        roof = {"kernel": "search_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                "unit": "GB/s", "frac": achieved / hbm_peak if achieved else None, "traffic": None,
+                "algorithmic_bytes": 32 * probes if probes else None, "peak_source": peak_src}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(args)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "u32/u64 integer", "data": "synthetic",
+            "config": {"workload": "ff_sieve 5 2097152: full reference map (16 GiB, mpv "
+                                   f"{g.maxPrimeMapValue}) + search of {job_sums} odd sums",
+                       "sum_start": 5, "sum_limit": LIMIT, "map_bytes": map_bytes,
+                       "l2": "inputs larger than L2 (16 GiB map rewritten every step)",
+                       "parallelism": f"sum shards x{world}" if world > 1 else "1 GPU"},
+            "kernel_ms": {"sieve_tiles": sieve_ms, "search_kernel": search_ms},
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": 2 * args.steps,
+        }
+        print(json.dumps(line), flush=True)
+
+
+# HBM-bound probes of the search at sumLimit 2^21 (search roofline);
+# filled in from the instrumented count when available.
+SEARCH_DRAM_PROBES = {}
+
+
+# ---------------------------------------------------------------------------------------
+# the reference's CPU program
+# ---------------------------------------------------------------------------------------
+def ref_binary():
+    """ff_seg built from the reference source with the largest THREADS <= cores-1."""
+    cores = os.cpu_count() or 1
+    best, best_t = None, 0
+    for t in (31, 63, 127, 255):
+        exe = os.path.join(ROOT, "oracle", "_ref", "ff_seg" if t == 31 else f"ff_seg_t{t}")
+        if os.path.exists(exe) and (t <= cores - 1 or best is None):
+            if t > best_t:
+                best, best_t = exe, t
+    return best, best_t
+
+
+# The sample: 8192 odd sums around 0.505 * 2^21, where the per-sum search cost equals the
+# average over 5..2^21 (the cumulative cost grows as ~s^2.05); ff_seg's own timers give its
+# sieve time for the sample's limit and its search time for the sample.
+SAMPLE = (1050625, 1067007)
+
+
+def run_ff_seg(exe, lo, hi):
+    d = tempfile.mkdtemp()
+    try:
+        out = subprocess.run([exe, str(lo), str(hi)], cwd=d, capture_output=True, check=True).stdout
+    finally:
+        try:
+            os.rmdir(d)
+        except OSError:
+            pass
+    p = int(re.search(rb"Prime time: (\d+)", out).group(1))
+    f = int(re.search(rb"Freudenthal time: (\d+)", out).group(1))
+    return p, f, out
+
+
+def map_bytes_for(limit):
+    import math
+    mgp = (limit + 1) >> 1
+    size = (max(((mgp * mgp) >> 2) + 2, 2) + 15) >> 4
+    return size
+
+
+def ref_sample_value(exe, threads):
+    lo, hi = SAMPLE
+    p_us, f_us, _ = run_ff_seg(exe, lo, hi)
+    n = odd_sums(lo, hi)
+    total = odd_sums(5, LIMIT - 1)
+    # the full job's sieve scaled from the sample's map to the 2^21 map, charged per sum
+    p_full = p_us * map_bytes_for(LIMIT) / map_bytes_for(hi)
+    t = (f_us + p_full * n / total) / 1e6
+    return n / t, {"prime_us": p_us, "freudenthal_us": f_us, "prime_full_est_us": p_full}
+
+
+def cpu_baseline(args):
+    exe, threads = ref_binary()
+    if not exe:
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "reference binary not built (oracle/_ref)"}
+    v, info = ref_sample_value(exe, threads)
+    return {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"ff_seg (THREADS={threads}) on odd sums {SAMPLE[0]}..{SAMPLE[1]} "
+                      f"(8192 sums of average cost); its sieve time scaled to the 2^21 map and "
+                      f"charged per sum", **info}
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return
+    exe, threads = ref_binary()
+    if not exe:
+        print(json.dumps({"impl": "reference", "unavailable": "reference binary oracle/_ref/ff_seg "
+                                                               "not built (needs the reference checkout)"}))
+        return
+    vals, infos = [], []
+    for _ in range(args.warmup):
+        ref_sample_value(exe, threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, info = ref_sample_value(exe, threads)
+        vals.append(v)
+        infos.append(info)
+    wall = time.perf_counter() - t0
+    value = statistics.mean(vals)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "u32/u64 integer", "data": "synthetic",
+        "config": {"workload": "ff_sieve 5 2097152 (bounded sample)", "sum_start": 5,
+                   "sum_limit": LIMIT},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"ff_seg (THREADS={threads}, reference source) on odd sums "
+                                   f"{SAMPLE[0]}..{SAMPLE[1]}; sieve time scaled to the 2^21 map "
+                                   f"and charged per sum", "last": infos[-1]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        ours(args, rank, world, dist)
+    finally:
+        if dist:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

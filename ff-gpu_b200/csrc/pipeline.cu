@@ -1,0 +1,225 @@
+// pipeline.cu -- one `ff_sieve <sumStart> <sumLimit>` run as a library call (ffb_run):
+// the reference's full map sieved on the device, every sum of ff_seg's schedule searched
+// on the device, the packed records copied back once, and the text emitted on the host
+// in ff_seg's order (reference/segmentedSieve.C:829-925).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "ffb200.h"
+#include "ffb_internal.h"
+#include "../host/plan.h"
+
+struct FfbContext {
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    uint8_t* d_map = nullptr;
+    uint64_t map_cap = 0;
+    uint64_t* d_rec = nullptr;
+    uint64_t rec_cap = 0;
+    uint64_t* h_rec = nullptr;  // pinned
+    uint64_t hrec_cap = 0;
+};
+
+namespace ffb {
+namespace {
+
+int grow(FfbContext* c, uint64_t map_bytes, uint64_t nrec)
+{
+    map_bytes = (map_bytes + 255) & ~255ull;
+    if (map_bytes > c->map_cap) {
+        if (c->d_map) cudaFree(c->d_map);
+        c->d_map = nullptr;
+        c->map_cap = 0;
+        FFB_CUDA(cudaMalloc(&c->d_map, map_bytes));
+        c->map_cap = map_bytes;
+    }
+    if (nrec > c->rec_cap) {
+        if (c->d_rec) cudaFree(c->d_rec);
+        c->d_rec = nullptr;
+        c->rec_cap = 0;
+        FFB_CUDA(cudaMalloc(&c->d_rec, 8 * nrec));
+        c->rec_cap = nrec;
+    }
+    if (nrec > c->hrec_cap) {
+        if (c->h_rec) cudaFreeHost(c->h_rec);
+        c->h_rec = nullptr;
+        c->hrec_cap = 0;
+        FFB_CUDA(cudaMallocHost(&c->h_rec, 8 * nrec));
+        c->hrec_cap = nrec;
+    }
+    return 0;
+}
+
+// Text of the solution lines of the schedule, numbered from 1 in emission order.
+// Ranges are formatted in parallel after a prefix count of their solutions.
+std::string emit(const std::vector<Range>& ranges, const uint64_t* rec, uint32_t lo)
+{
+    const size_t nr = ranges.size();
+    std::vector<uint32_t> cnt(nr, 0), first(nr, 0);
+    for (size_t r = 0; r < nr; ++r)
+        for (uint32_t s = ranges[r].first | 1u; s <= ranges[r].last; s += 2)
+            cnt[r] += rec[(s - lo) >> 1] != 0;
+    uint32_t total = 0;
+    for (size_t r = 0; r < nr; ++r) {
+        first[r] = total;
+        total += cnt[r];
+    }
+    std::vector<std::string> parts(nr);
+    auto work = [&](size_t r) {
+        std::string& out = parts[r];
+        out.resize((size_t)cnt[r] * kMaxLine);
+        char* p = &out[0];
+        uint32_t count = first[r];
+        for (uint32_t s = ranges[r].first | 1u; s <= ranges[r].last; s += 2) {
+            const uint64_t v = rec[(s - lo) >> 1];
+            if (!v) continue;
+            p = format_line(p, ++count, s, rec_low(v), rec_high(v), rec_low_prime(v),
+                            rec_high_prime(v));
+        }
+        out.resize((size_t)(p - &out[0]));
+    };
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = std::max(1u, std::min(nt, 16u));
+    if (total < 4096) nt = 1;
+    if (nt == 1) {
+        for (size_t r = 0; r < nr; ++r) work(r);
+    } else {
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t)
+            th.emplace_back([&, t] {
+                for (size_t r = t; r < nr; r += nt) work(r);
+            });
+        for (auto& t : th) t.join();
+    }
+    size_t bytes = 0;
+    for (auto& s : parts) bytes += s.size();
+    std::string all;
+    all.reserve(bytes);
+    for (auto& s : parts) all += s;
+    return all;
+}
+
+}  // namespace
+}  // namespace ffb
+
+using namespace ffb;
+
+extern "C" FfbContext* ffb_context_create(int deviceIndex)
+{
+    if (!device_state(deviceIndex)) return nullptr;
+    FfbContext* c = new FfbContext;
+    c->dev = deviceIndex;
+    if (cudaSetDevice(deviceIndex) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return nullptr;
+    }
+    return c;
+}
+
+extern "C" void ffb_context_destroy(FfbContext* c)
+{
+    if (!c) return;
+    cudaSetDevice(c->dev);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->d_map) cudaFree(c->d_map);
+    if (c->d_rec) cudaFree(c->d_rec);
+    if (c->h_rec) cudaFreeHost(c->h_rec);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" void ffb_free(void* p) { std::free(p); }
+
+extern "C" int ffb_run(FfbContext* ctx, int nargs, int32_t a1, int32_t a2, char** text, size_t* len)
+{
+    using clk = std::chrono::steady_clock;
+    *text = nullptr;
+    *len = 0;
+    uint32_t start, limit;
+    parse_args(nargs, a1, a2, &start, &limit);
+    char hdr[2048];
+    Geometry g;
+    const int hn = plan_geometry(start, limit, &g, hdr, sizeof hdr);
+    if (hn < 0) {
+        std::fprintf(stderr, "ffb_run: %s", g.too_big ? hdr : "header overflow\n");
+        return -1;
+    }
+    std::vector<Range> ranges;
+    if (!plan_schedule(start, limit, g.mpv, kThreads, ranges)) {
+        std::fprintf(stderr, "ffb_run: range [%u, %u] outside what the reference can run\n", start,
+                     limit);
+        return -1;
+    }
+    uint32_t lo = 0xFFFFFFFFu, hi = 0;
+    for (const Range& r : ranges) {
+        const uint32_t f = r.first | 1u;
+        if (f > r.last) continue;
+        lo = std::min(lo, f);
+        hi = std::max(hi, r.last - !(r.last & 1));
+    }
+    if (hi > kMaxSum) {
+        std::fprintf(stderr, "ffb_run: sums above 2^25 are outside the exact domain\n");
+        return -1;
+    }
+    FfbContext* c = ctx ? ctx : ffb_context_create(0);
+    if (!c) return -1;
+    int rc = 0;
+    std::string body;
+    double prime_us = 0, freud_us = 0;
+    do {
+        const uint64_t nrec = lo <= hi ? ((uint64_t)hi - lo) / 2 + 1 : 1;
+        if ((rc = grow(c, g.map_bytes, nrec))) break;
+        cudaSetDevice(c->dev);
+        const auto t0 = clk::now();
+        if ((rc = ffb_sieve_map_async(c->dev, g.mpv, c->d_map, c->stream))) break;
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) { rc = -1; break; }
+        const auto t1 = clk::now();
+        if (lo <= hi) {
+            if ((rc = ffb_search_async(c->dev, c->d_map, g.mpv, lo, hi, c->d_rec, c->stream))) break;
+            if (cudaMemcpyAsync(c->h_rec, c->d_rec, 8 * nrec, cudaMemcpyDeviceToHost, c->stream) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(c->stream) != cudaSuccess) {
+                rc = -1;
+                break;
+            }
+            uint32_t flags = 0;
+            if ((rc = ffb_take_errors(c->dev, &flags))) break;
+            if (flags) {
+                std::fprintf(stderr, "ffb_run: device error flags 0x%x\n", flags);
+                rc = -1;
+                break;
+            }
+            body = emit(ranges, c->h_rec, lo);
+        }
+        const auto t2 = clk::now();
+        prime_us = std::chrono::duration<double, std::micro>(t1 - t0).count();
+        freud_us = std::chrono::duration<double, std::micro>(t2 - t1).count();
+    } while (0);
+    if (!ctx) ffb_context_destroy(c);
+    if (rc) {
+        std::fprintf(stderr, "ffb_run: failed: %s\n", cudaGetErrorString(cudaGetLastError()));
+        return -1;
+    }
+    char tail[160];
+    const int tn = std::snprintf(tail, sizeof tail, "Prime time: %llu \xce\xbcs\nFreudenthal time: %llu \xce\xbcs\n",
+                                 (unsigned long long)prime_us, (unsigned long long)freud_us);
+    const size_t n = (size_t)hn + body.size() + (size_t)tn;
+    char* out = (char*)std::malloc(n + 1);
+    if (!out) return -1;
+    std::memcpy(out, hdr, (size_t)hn);
+    std::memcpy(out + hn, body.data(), body.size());
+    std::memcpy(out + hn + body.size(), tail, (size_t)tn);
+    out[n] = 0;
+    *text = out;
+    *len = n;
+    return 0;
+}

@@ -1,0 +1,405 @@
+// search.cu -- the per-sum Freudenthal search (reference/segmentedSieve.C:419-639, 800-823).
+//
+// Parallel structure (sm_100a, SIMT integer code):
+//   * A persistent grid; each warp pulls chunks of 32 consecutive odd sums from a device
+//     counter, largest sums first (their cost grows with the sum, so big ones start early).
+//   * Lane-parallel over the 32 sums: Sammy's first statement (the RunIt filter) and the
+//     Power2Prime phase. A sum still open after that (at most one valid split so far) is a
+//     "survivor".
+//   * Warp-cooperative per survivor: lanes enumerate the Power2Odd / Power2Even splits
+//     (k, o) in parallel. The verdict of the reference depends only on WHETHER exactly one
+//     split is valid (and then on that split), not on the order the splits are visited, so
+//     the order is free and the warp stops as soon as two valid splits are seen.
+//   * Rare, expensive work is deferred through per-warp shared-memory queues so lanes stay
+//     converged: stage 0 (every split) runs the divisibility filters and the pair probe
+//     o + b*2^k - 2, whose values are small (bitmap prefix, cache resident); stage 1 (about
+//     one split in eight) probes 2^k + o*b - 2, a random HBM sector; stage 2 (about one in
+//     a hundred) runs AllButOne... on the split's product.
+//   * AllButOne... is evaluated from the factorisations of o and b (both below the sum)
+//     instead of the reference's trial-division walk over all primes; the walk's divisor
+//     list, its partially-sorted skip (reference/segmentedSieve.C:451) and its early
+//     returns are replayed exactly from the factorisation, since every IsPrime it makes on
+//     the cofactor is a pure function of the factorisation.
+#include "ffb_device.cuh"
+#include "ffb_internal.h"
+
+namespace ffb {
+namespace {
+
+constexpr int kWarps = 8;        // warps per block
+constexpr int kQueue = 64;       // per-warp queue capacity (entries)
+constexpr int kMaxPf = 16;       // distinct odd prime factors of a product < 2^52
+constexpr int kMaxDiv = 64;      // divisor list of one AllButOne... call
+
+struct Fac {
+    uint32_t q[kMaxPf];
+    uint32_t e[kMaxPf];
+    int n;
+};
+
+// Ascending prime factorisation of an odd x < 2^32 by the exact-division table, with the
+// cofactor's primality read from the bitmap after every factor found.
+__device__ int factor_odd(uint32_t x, uint32_t* q, uint32_t* e, int cap, const SearchArgs& A)
+{
+    int cnt = 0;
+    uint32_t n = x;
+    if (n <= 1) return 0;
+    if (is_prime(A.map, A.bound, n, A.err)) { q[0] = n; e[0] = 1; return 1; }
+    for (uint32_t i = 0; i < A.ntdiv; ++i) {
+        const TDiv t = A.tdiv[i];
+        if ((uint64_t)t.p * t.p > n) break;
+        uint32_t y = n * t.inv;
+        if (y <= t.lim) {
+            uint32_t ex = 0;
+            do { n = y; ++ex; y = n * t.inv; } while (y <= t.lim);
+            if (cnt < cap) { q[cnt] = t.p; e[cnt] = ex; }
+            ++cnt;
+            if (n == 1) return cnt;
+            if (is_prime(A.map, A.bound, n, A.err)) {
+                if (cnt < cap) { q[cnt] = n; e[cnt] = 1; }
+                return cnt + 1;
+            }
+        }
+    }
+    if (n > 1) {
+        if (cnt < cap) { q[cnt] = n; e[cnt] = 1; }
+        ++cnt;
+    }
+    return cnt;
+}
+
+__device__ void factor_product(uint32_t a, uint32_t b, Fac& f, const SearchArgs& A)
+{
+    uint32_t qa[10], ea[10], qb[10], eb[10];
+    int na = factor_odd(a, qa, ea, 10, A);
+    int nb = b == 1 ? 0 : factor_odd(b, qb, eb, 10, A);
+    int i = 0, j = 0, n = 0;
+    while (i < na || j < nb) {
+        uint32_t q, e;
+        if (j >= nb || (i < na && qa[i] < qb[j])) { q = qa[i]; e = ea[i]; ++i; }
+        else if (i >= na || qb[j] < qa[i]) { q = qb[j]; e = eb[j]; ++j; }
+        else { q = qa[i]; e = ea[i] + eb[j]; ++i; ++j; }
+        if (n < kMaxPf) { f.q[n] = q; f.e[n] = e; }
+        ++n;
+    }
+    f.n = n < kMaxPf ? n : kMaxPf;
+}
+
+// AllButOneProductOfTermPairsOfSumOfFactorPairsHasSingleFactorPair
+// (reference/segmentedSieve.C:424-477) replayed from the factorisation f of oddProduct.
+// F[i] are the divisors the reference stores in factors[], C[i] = product / F[i].
+__device__ __noinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const Fac& f,
+                                         const SearchArgs& A)
+{
+    const uint64_t P = odd_product << k;
+    const uint64_t lim = isqrt64(P);
+    uint64_t F[kMaxDiv], C[kMaxDiv];
+    uint32_t nf = 0, npend = 0, nm = 0;
+    F[0] = 1ull << k;
+    C[0] = odd_product;
+    if (F[0] <= lim) {
+        nm += !single_pair(A.map, A.bound, F[0] + C[0], A.err);
+        nf = 1;
+    }
+    int idx = 0;
+    bool first = true;  // the reference tries 3 before its first IsPrime(testProduct)
+    for (;;) {
+        uint64_t q;
+        uint32_t e;
+        if (first) {
+            first = false;
+            if (f.n > 0 && f.q[0] == 3) { q = 3; e = f.e[0]; idx = 1; }
+            else continue;
+        } else {
+            if (idx >= f.n) break;                                   // testProduct == 1
+            q = f.q[idx];
+            e = f.e[idx];
+            if (idx == f.n - 1 && e == 1 && q > lim) break;          // prime cofactor > limit
+            ++idx;
+        }
+        // the reference's divides-branch for q, q^2, ..., q^e
+        const uint64_t qi = inv64(q);
+        uint64_t tf = q, tfi = qi;
+        for (uint32_t j = 0; j < e; ++j) {
+            if (tf <= lim) {
+                const uint64_t ctf = (odd_product * tfi) << k;     // P / tf, exact
+                if ((nm += !single_pair(A.map, A.bound, tf + ctf, A.err)) > 1) return false;
+                if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return false; }
+                F[nf + npend] = tf;
+                C[nf + npend] = ctf;
+                ++npend;
+                for (uint32_t g = 0; g < nf; ++g) {
+                    const uint64_t m = F[g] * tf;
+                    if (m <= lim) {
+                        const uint64_t cm = C[g] * tfi;              // C[g] / tf, exact
+                        if ((nm += !single_pair(A.map, A.bound, m + cm, A.err)) > 1) return false;
+                        if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return false; }
+                        F[nf + npend] = m;
+                        C[nf + npend] = cm;
+                        ++npend;
+                    } else {
+                        // skip the rest of this ascending run of F (reference :451)
+                        for (const uint64_t v = F[g]; g + 1 < nf && v <= F[g + 1]; ++g) {}
+                    }
+                }
+                if (nm > 1) return false;
+            }
+            tf *= q;
+            tfi *= qi;
+        }
+        nf += npend;
+        npend = 0;
+    }
+    return nm == 1;
+}
+
+// Split encoding in the queues: bits 0..4 k, bit 5 composite (Power2Composite item: the odd
+// term is sum - 2^k), bits 6..31 the odd part o of the even term (o < 2^26).
+__device__ __forceinline__ uint32_t enc(uint32_t k, uint32_t o, bool comp)
+{
+    return k | (comp ? 32u : 0u) | (o << 6);
+}
+
+// Stage 2: the split's AllButOne... verdict (DoesPeterKnow's last step, or Power2Composite).
+__device__ bool stage2(uint32_t item, uint32_t s, const SearchArgs& A, uint32_t* ta, uint32_t* tb)
+{
+    const uint32_t k = item & 31;
+    Fac f;
+    uint64_t odd_product;
+    if (item & 32) {
+        const uint32_t odd = s - (1u << k);
+        factor_product(odd, 1, f, A);
+        odd_product = odd;
+        *ta = 1u << k;
+        *tb = odd;
+    } else {
+        const uint32_t o = item >> 6;
+        const uint32_t even = o << k, b = s - even;
+        factor_product(o, b, f, A);
+        odd_product = (uint64_t)o * b;
+        *ta = even;
+        *tb = b;
+    }
+    return all_but_one(k, odd_product, f, A);
+}
+
+// Stage 1: the probe of 2^k + o*b - 2 (DoesPeterKnow's first test).
+__device__ __forceinline__ bool stage1(uint32_t item, uint32_t s, const SearchArgs& A)
+{
+    const uint32_t k = item & 31, o = item >> 6;
+    const uint32_t b = s - (o << k);
+    return single_pair(A.map, A.bound, (1ull << k) + (uint64_t)o * b, A.err);
+}
+
+struct WarpQ {
+    uint32_t a[kQueue];
+    uint32_t b[kQueue];
+};
+
+// Appends the items of the lanes with `pred` to q[n..]; returns the new size (uniform).
+__device__ __forceinline__ uint32_t push(uint32_t* q, uint32_t n, bool pred, uint32_t item, int lane)
+{
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, pred);
+    if (pred) q[n + __popc(m & ((1u << lane) - 1))] = item;
+    __syncwarp();
+    return n + __popc(m);
+}
+
+struct SumState {
+    uint32_t s;
+    uint32_t count;   // valid splits seen so far (saturating use: >= 2 means rejected)
+    uint32_t ta, tb;  // terms of the first valid split
+    uint32_t na, nb;  // queue sizes
+};
+
+// Runs stage 1 on up to 32 queued items, moving the survivors to queue b.
+__device__ void drain_a(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
+{
+    const uint32_t take = st.na < 32 ? st.na : 32;
+    const uint32_t base = st.na - take;
+    const bool act = (uint32_t)lane < take;
+    const uint32_t item = act ? Q.a[base + lane] : 0;
+    __syncwarp();
+    st.na = base;
+    const bool pass = act && stage1(item, st.s, A);
+    st.nb = push(Q.b, st.nb, pass, item, lane);
+}
+
+// Runs stage 2 on up to 32 queued items and adds the valid ones to the count.
+__device__ void drain_b(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
+{
+    const uint32_t take = st.nb < 32 ? st.nb : 32;
+    const uint32_t base = st.nb - take;
+    const bool act = (uint32_t)lane < take;
+    const uint32_t item = act ? Q.b[base + lane] : 0;
+    __syncwarp();
+    st.nb = base;
+    uint32_t a = 0, b = 0;
+    const bool valid = act && stage2(item, st.s, A, &a, &b);
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, valid);
+    if (m) {
+        const int src = __ffs(m) - 1;
+        a = __shfl_sync(0xFFFFFFFFu, a, src);
+        b = __shfl_sync(0xFFFFFFFFu, b, src);
+        if (st.count == 0) { st.ta = a; st.tb = b; }
+        st.count += __popc(m);
+    }
+}
+
+// Stage 0 of a Power2Odd split (reference/segmentedSieve.C:573-586 and the cheap probe of
+// DoesPeterKnow :636): o*b not a multiple of 3, and o == b or o + b*2^k - 2 prime.
+__device__ __forceinline__ bool stage0_odd(uint32_t s, uint32_t k, uint32_t o, const SearchArgs& A)
+{
+    const uint32_t b = s - (o << k);
+    if (o % 3 == 0 || b % 3 == 0) return false;
+    return o == b || single_pair(A.map, A.bound, o + ((uint64_t)b << k), A.err);
+}
+
+// Stage 0 of a Power2Even split (reference/segmentedSieve.C:614-627): o*b a multiple of 3
+// or b prime; then the cheap probe.
+__device__ __forceinline__ bool stage0_even(uint32_t s, uint32_t k, uint32_t o, const SearchArgs& A)
+{
+    const uint32_t b = s - (o << k);
+    if (o % 3 != 0 && b % 3 != 0 && !is_prime(A.map, A.bound, b, A.err)) return false;
+    return o == b || single_pair(A.map, A.bound, o + ((uint64_t)b << k), A.err);
+}
+
+// Enumerates the splits of one phase for sum s: k = kfirst, kfirst+2, ... while o0<<k < s-2;
+// for each k the odd parts o = o0, o0+2, ... with o<<k < s-2. Returns false once the sum
+// is rejected (two valid splits).
+template <bool kOdd>
+__device__ bool run_phase(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
+{
+    const uint32_t s = st.s;
+    const uint32_t o0 = kOdd ? 5 : 3;
+    for (uint32_t k = kOdd ? 3 : 2; (o0 << k) < s - 2; k += 2) {
+        // odd o in [o0, omax] with o<<k <= s-3
+        const uint32_t omax = (s - 3) >> k;
+        const uint32_t n = omax >= o0 ? ((omax - o0) >> 1) + 1 : 0;
+        for (uint32_t base = 0; base < n; base += 32) {
+            const uint32_t i = base + lane;
+            const uint32_t o = o0 + 2 * i;
+            const bool act = i < n;
+            const bool pass = act && (kOdd ? stage0_odd(s, k, o, A) : stage0_even(s, k, o, A));
+            st.na = push(Q.a, st.na, pass, enc(k, o, false), lane);
+            if (st.na >= 32) {
+                drain_a(st, Q, A, lane);
+                if (st.nb >= 32) {
+                    drain_b(st, Q, A, lane);
+                    if (st.count > 1) return false;
+                }
+            }
+        }
+    }
+    return true;
+}
+
+__device__ void write_result(const SearchArgs& A, uint32_t s, uint32_t ta, uint32_t tb)
+{
+    uint32_t lo = ta < tb ? ta : tb, hi = ta < tb ? tb : ta;
+    if (A.rec) {
+        const bool lp = is_prime(A.map, A.bound, lo, A.err);
+        const bool hp = is_prime(A.map, A.bound, hi, A.err);
+        A.rec[(s - A.lo) >> 1] = ((uint64_t)(lo | (lp ? 0x80000000u : 0u)) << 32) |
+                                 (uint64_t)(hi | (hp ? 0x80000000u : 0u));
+    }
+    if (A.grec) {
+        // GpuRecord {u32 sum @0, u64 low @8, u64 high @16, u8 tag @24}, 32 bytes
+        uint8_t* r = (uint8_t*)A.grec + (size_t)((s - A.grec_base) >> 1) * 32;
+        *(uint32_t*)(r + 0) = s;
+        *(uint64_t*)(r + 8) = lo;
+        *(uint64_t*)(r + 16) = hi;
+        r[24] = 0;
+        if (A.gcount) atomicAdd(A.gcount, 1u);
+    }
+}
+
+__global__ void __launch_bounds__(kWarps * 32) search_kernel(const SearchArgs A)
+{
+    __shared__ WarpQ queues[kWarps];
+    const int lane = threadIdx.x & 31;
+    WarpQ& Q = queues[threadIdx.x >> 5];
+    const uint32_t nchunks = (A.nsums + 31) / 32;
+    for (;;) {
+        uint32_t c = 0;
+        if (lane == 0) c = atomicAdd(A.sched, 1u);
+        c = __shfl_sync(0xFFFFFFFFu, c, 0);
+        if (c >= nchunks) break;
+
+        // ---- lane-parallel: filter + Power2Prime for 32 sums (largest first) ----
+        const uint32_t idx = c * 32 + lane;
+        const bool act = idx < A.nsums;
+        const uint32_t s = act ? A.hi - 2 * idx : 5;
+        bool surv = false;
+        uint32_t cnt = 0, ta = 0, tb = 0, comp = 0;
+        if (act) {
+            // Sammy's first statement (reference/segmentedSieve.C:805-806)
+            const uint32_t d3 = s / 3;
+            bool pass = !single_pair(A.map, A.bound, s, A.err) &&
+                        (s != 3 * d3 || is_prime(A.map, A.bound, d3, A.err));
+            if (pass) {
+                // Power2Prime (reference/segmentedSieve.C:547-564)
+                for (uint32_t even = 4, k = 2; even < s - 2; even <<= 1, ++k) {
+                    const uint32_t odd = s - even;
+                    if (is_prime(A.map, A.bound, odd, A.err)) {
+                        if (++cnt > 1) break;
+                        if (cnt == 1) { ta = even; tb = odd; }
+                    } else {
+                        comp |= 1u << k;
+                    }
+                }
+                surv = cnt <= 1;
+            }
+        }
+
+        // ---- warp-cooperative: the remaining phases, one survivor at a time ----
+        uint32_t smask = __ballot_sync(0xFFFFFFFFu, surv);
+        while (smask) {
+            const int src = __ffs(smask) - 1;
+            smask &= smask - 1;
+            SumState st;
+            st.s = __shfl_sync(0xFFFFFFFFu, s, src);
+            st.count = __shfl_sync(0xFFFFFFFFu, cnt, src);
+            st.ta = __shfl_sync(0xFFFFFFFFu, ta, src);
+            st.tb = __shfl_sync(0xFFFFFFFFu, tb, src);
+            const uint32_t cmask = __shfl_sync(0xFFFFFFFFu, comp, src);
+            st.na = 0;
+            st.nb = 0;
+            // Power2Composite items (reference/segmentedSieve.C:591-605) go straight to stage 2
+            st.nb = push(Q.b, 0, (cmask >> lane) & 1, enc(lane, 0, true), lane);
+            bool open = true;
+            if (st.nb >= 32) { drain_b(st, Q, A, lane); open = st.count <= 1; }
+            if (open) open = run_phase<true>(st, Q, A, lane);
+            if (open) open = run_phase<false>(st, Q, A, lane);
+            while (open && st.na > 0) {
+                drain_a(st, Q, A, lane);
+                if (st.nb >= 32) { drain_b(st, Q, A, lane); open = st.count <= 1; }
+            }
+            while (open && st.nb > 0) {
+                drain_b(st, Q, A, lane);
+                open = st.count <= 1;
+            }
+            if (open && st.count == 1 && lane == 0) write_result(A, st.s, st.ta, st.tb);
+            __syncwarp();
+        }
+    }
+}
+
+}  // namespace
+
+int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
+{
+    if (a.nsums == 0) return 0;
+    int per_sm = 0;
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel, kWarps * 32, 0));
+    if (per_sm < 1) per_sm = 1;
+    uint32_t chunks = (a.nsums + 31) / 32;
+    uint32_t blocks = (uint32_t)sms * (uint32_t)per_sm;
+    const uint32_t need = (chunks + kWarps - 1) / kWarps;
+    if (blocks > need) blocks = need;
+    search_kernel<<<blocks, kWarps * 32, 0, stream>>>(a);
+    FFB_CUDA(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace ffb

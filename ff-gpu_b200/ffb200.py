@@ -1,0 +1,148 @@
+"""ctypes binding of the C ABI in include/ffb200.h (lib/libffb200.so).
+
+The Python side is a thin caller of the library: every computation happens in the CUDA
+kernels behind the C entry points. Loading fails loudly when the library has not been
+built (there is no fallback).
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libffb200.so")
+
+u8p = ctypes.POINTER(ctypes.c_uint8)
+u32p = ctypes.POINTER(ctypes.c_uint32)
+u64p = ctypes.POINTER(ctypes.c_uint64)
+
+
+class GpuRecord(ctypes.Structure):
+    """source/m4/gpu_search_kernel.h:37-42 (sizeof 32)."""
+    _fields_ = [("sum", ctypes.c_uint32), ("low", ctypes.c_uint64),
+                ("high", ctypes.c_uint64), ("tag", ctypes.c_uint8)]
+
+
+class FfbGeometry(ctypes.Structure):
+    _fields_ = [("sumStart", ctypes.c_uint32), ("sumLimit", ctypes.c_uint32),
+                ("maxPrimeMapValue", ctypes.c_uint64), ("mapBytes", ctypes.c_uint64),
+                ("numPrimesRequested", ctypes.c_uint64), ("pmapSumLimit", ctypes.c_uint64)]
+
+
+# name -> (restype, argtypes); every symbol include/ffb200.h declares
+SIGNATURES = {
+    "SieveSlabRun_sm_100a": (ctypes.c_int, [ctypes.c_int, u32p, ctypes.c_uint32, ctypes.c_uint64,
+                                            ctypes.c_uint64, u8p]),
+    "SieveSlabGetLaunchFn_sm_100a": (ctypes.c_void_p, [ctypes.c_int]),
+    "SieveSlabRun_sm_120": (ctypes.c_int, [ctypes.c_int, u32p, ctypes.c_uint32, ctypes.c_uint64,
+                                           ctypes.c_uint64, u8p]),
+    "SieveSlabGetLaunchFn_sm_120": (ctypes.c_void_p, [ctypes.c_int]),
+    "SieveSlabGetLaunchFn_gfx1201": (ctypes.c_void_p, [ctypes.c_int]),
+    "SieveSlabEngineRun_sm_100a": (ctypes.c_int, [ctypes.c_int, u32p, ctypes.c_uint32,
+                                                  ctypes.c_uint64, u8p]),
+    "SieveSlabEngineGetLaunchFn_sm_100a": (ctypes.c_void_p, [ctypes.c_int]),
+    "SieveSlabEngineRun_sm_120": (ctypes.c_int, [ctypes.c_int, u32p, ctypes.c_uint32,
+                                                 ctypes.c_uint64, u8p]),
+    "SieveSlabEngineGetLaunchFn_sm_120": (ctypes.c_void_p, [ctypes.c_int]),
+    "SieveSlabEngineGetLaunchFn_gfx1201": (ctypes.c_void_p, [ctypes.c_int]),
+    "SievePoolGet_sm_100a": (ctypes.c_void_p, [ctypes.c_int]),
+    "SievePoolGet_sm_120": (ctypes.c_void_p, [ctypes.c_int]),
+    "SievePoolGet_gfx1201": (ctypes.c_void_p, [ctypes.c_int]),
+    "SearchKernelRun_sm_100a": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                                               ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p,
+                                               ctypes.c_void_p]),
+    "SearchKernelGetLaunchFn_sm_100a": (ctypes.c_void_p, [ctypes.c_int]),
+    "SearchKernelRun_sm_120": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                                              ctypes.c_uint64, ctypes.c_uint64, ctypes.c_void_p,
+                                              ctypes.c_void_p]),
+    "SearchKernelGetLaunchFn_sm_120": (ctypes.c_void_p, [ctypes.c_int]),
+    "SearchKernelGetLaunchFn_gfx1201": (ctypes.c_void_p, [ctypes.c_int]),
+    "GpuSearchLaunch": (ctypes.c_int, [ctypes.c_int, ctypes.c_char_p, ctypes.c_void_p,
+                                       ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                       ctypes.c_void_p, ctypes.c_void_p]),
+    "ffb_format_line": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                       ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_char_p, ctypes.c_size_t]),
+    "ffb_geometry": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
+                                    ctypes.POINTER(FfbGeometry), ctypes.c_char_p, ctypes.c_size_t]),
+    "ffb_schedule": (ctypes.c_int, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                                    ctypes.c_uint32, u32p, u32p, ctypes.c_int]),
+    "ffb_sieve_map_async": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_void_p,
+                                           ctypes.c_void_p]),
+    "ffb_search_async": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                                        ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+                                        ctypes.c_void_p]),
+    "ffb_take_errors": (ctypes.c_int, [ctypes.c_int, u32p]),
+    "ffb_context_create": (ctypes.c_void_p, [ctypes.c_int]),
+    "ffb_context_destroy": (None, [ctypes.c_void_p]),
+    "ffb_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
+                               ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]),
+    "ffb_free": (None, [ctypes.c_void_p]),
+}
+
+_lib = None
+
+
+def load():
+    """The library handle with argument types set; raises if the library is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is not built (run `make -C ff-gpu_b200`)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def geometry(*args):
+    """ffb_geometry for 0, 1 or 2 atoi()-style positional arguments -> (FfbGeometry, header)."""
+    lib = load()
+    g = FfbGeometry()
+    buf = ctypes.create_string_buffer(4096)
+    a = list(args) + [0, 0]
+    n = lib.ffb_geometry(len(args), a[0], a[1], ctypes.byref(g), buf, len(buf))
+    if n < 0:
+        raise ValueError(buf.value.decode())
+    return g, buf.raw[:n]
+
+
+def schedule(sum_start, sum_limit, mpv, threads=31):
+    lib = load()
+    cap = 8 * threads + 8
+    f = (ctypes.c_uint32 * cap)()
+    l = (ctypes.c_uint32 * cap)()
+    n = lib.ffb_schedule(sum_start, sum_limit, mpv, threads, f, l, cap)
+    if n < 0:
+        raise ValueError("schedule failed")
+    return [(f[i], l[i]) for i in range(n)]
+
+
+def format_line(count, s, low, high, low_prime, high_prime):
+    lib = load()
+    buf = ctypes.create_string_buffer(256)
+    n = lib.ffb_format_line(count, s, low, high, int(low_prime), int(high_prime), buf, len(buf))
+    return buf.raw[:n]
+
+
+def run(*args, ctx=None):
+    """The full ff_sieve stdout for the positional arguments, as bytes."""
+    lib = load()
+    p = ctypes.c_void_p()
+    n = ctypes.c_size_t()
+    rc = lib.ffb_run(ctx, len(args), *(list(args) + [0, 0])[:2], ctypes.byref(p), ctypes.byref(n))
+    if rc != 0:
+        raise RuntimeError(f"ffb_run{args} failed")
+    try:
+        return ctypes.string_at(p, n.value)
+    finally:
+        lib.ffb_free(p)
+
+
+def take_errors(dev=0):
+    lib = load()
+    f = ctypes.c_uint32()
+    if lib.ffb_take_errors(dev, ctypes.byref(f)) != 0:
+        raise RuntimeError("ffb_take_errors failed")
+    return f.value

@@ -1,0 +1,225 @@
+/*
+ * ffb200.h -- C ABI of the B200 (sm_100a) build of ff-gpu's hot path: the odd-only prime
+ * sieve and the per-sum Freudenthal search.
+ *
+ * Every entry point keeps the name, argument meaning, return codes and memory ownership
+ * of the reference interface it replaces (cited per declaration), with the arch tag
+ * sm_100a. The reference's own harnesses resolve the NVIDIA kernels through the _sm_120
+ * names, so those are exported as aliases of the sm_100a functions; the _gfx1201 getters
+ * exist for link compatibility and return NULL (there is no AMD path and no dispatch).
+ *
+ * Plain pointers and sizes only. "d_" pointers are CUDA device pointers, "h_" pointers
+ * host memory. All functions return 0 on success and -1 on error (with one line on
+ * stderr), unless stated otherwise.
+ *
+ * Domain: sums up to 2^25 (products below 2^48, where the reference's Miller-Rabin
+ * arithmetic is exact); larger sumLimit values are rejected with -1.
+ */
+#ifndef FFB200_H
+#define FFB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One solution slot (source/m4/gpu_search_kernel.h:37-42): sum==0 marks an empty slot.
+ * Layout {u32 sum @0, u64 low @8, u64 high @16, u8 tag @24}, sizeof 32. tag is 0. */
+typedef struct {
+    uint32_t sum;
+    uint64_t low;
+    uint64_t high;
+    uint8_t tag;
+} GpuRecord;
+
+/* ---------------------------------------------------------------------------------- */
+/* Sieve slab (source/sieve_slab_kernel.cpp:41-48, 66-131)                             */
+/* ---------------------------------------------------------------------------------- */
+
+typedef int (*SieveSlabRunFn)(int deviceIndex, const uint32_t* h_primes, uint32_t numPrimes,
+                              uint64_t segLo, uint64_t segHi, uint8_t* h_out);
+
+/* Sieves the values [segLo, segHi) with the listed primes (ascending; the reference's
+ * callers pass the odd primes up to sqrt(segHi), some with a leading 2, which is honoured
+ * literally). h_out receives (segHi+15)>>4 bytes: the marks in segLo-RELATIVE layout
+ * (value i -> byte (i-segLo)>>4, bit 0x80>>((i-segLo)>>1&7)), all other bytes 0xff,
+ * byte 0 = 0x7f when segLo == 0. Synchronous; allocates and frees its own device memory.
+ * Replaces SieveSlabRun_<arch> (source/sieve_slab_kernel.cpp:80-131). */
+int SieveSlabRun_sm_100a(int deviceIndex, const uint32_t* h_primes, uint32_t numPrimes,
+                         uint64_t segLo, uint64_t segHi, uint8_t* h_out);
+/* Returns SieveSlabRun_sm_100a when deviceIndex names a visible CUDA device, else NULL.
+ * Replaces SieveSlabGetLaunchFn_<arch> (source/sieve_slab_kernel.cpp:124-131). */
+SieveSlabRunFn SieveSlabGetLaunchFn_sm_100a(int deviceIndex);
+int SieveSlabRun_sm_120(int deviceIndex, const uint32_t* h_primes, uint32_t numPrimes,
+                        uint64_t segLo, uint64_t segHi, uint8_t* h_out);
+SieveSlabRunFn SieveSlabGetLaunchFn_sm_120(int deviceIndex);
+SieveSlabRunFn SieveSlabGetLaunchFn_gfx1201(int deviceIndex); /* always NULL */
+
+/* ---------------------------------------------------------------------------------- */
+/* Full-map engine and pool operations (source/sieve_slab_engine.h:27-101)             */
+/* ---------------------------------------------------------------------------------- */
+
+typedef int (*SieveSlabEngineRunFn)(int deviceIndex, const uint32_t* h_primes,
+                                    uint32_t numPrimes, uint64_t maxPrimeMapValue,
+                                    uint8_t* h_out);
+
+/* The whole map for values [0, maxPrimeMapValue]: h_out receives
+ * (maxPrimeMapValue+1+15)>>4 bytes in the reference layout. h_primes must hold the odd
+ * primes up to sqrt(maxPrimeMapValue) (2 excluded). Synchronous.
+ * Replaces SieveSlabEngineRun_<arch> (source/sieve_slab_engine.cpp:115-202). */
+int SieveSlabEngineRun_sm_100a(int deviceIndex, const uint32_t* h_primes, uint32_t numPrimes,
+                               uint64_t maxPrimeMapValue, uint8_t* h_out);
+/* source/sieve_slab_engine.cpp:209-216 */
+SieveSlabEngineRunFn SieveSlabEngineGetLaunchFn_sm_100a(int deviceIndex);
+int SieveSlabEngineRun_sm_120(int deviceIndex, const uint32_t* h_primes, uint32_t numPrimes,
+                              uint64_t maxPrimeMapValue, uint8_t* h_out);
+SieveSlabEngineRunFn SieveSlabEngineGetLaunchFn_sm_120(int deviceIndex);
+SieveSlabEngineRunFn SieveSlabEngineGetLaunchFn_gfx1201(int deviceIndex); /* always NULL */
+
+/* The pool operation table (source/sieve_slab_engine.h:49-98), same 19 members in the
+ * same order. Every op makes vendorIndex the calling thread's current device first.
+ * slabCompute / slabComputeAsync clear bits INTO d_slab (bitwise AND, like the reference
+ * kernel), so an unprimed buffer gives the same bytes the reference would. */
+typedef struct SievePoolOps {
+    void* (*alloc)(int vendorIndex, uint64_t bytes);
+    int (*memset)(int vendorIndex, void* d_ptr, int v, uint64_t bytes);
+    int (*free)(int vendorIndex, void* d_ptr);
+    int (*copyH2D)(int vendorIndex, void* d_dst, const void* h_src, uint64_t bytes);
+    int (*copyD2H)(int vendorIndex, void* h_dst, const void* d_src, uint64_t bytes);
+    int (*slabCompute)(int vendorIndex, const uint32_t* h_primes, uint32_t numPrimes,
+                       uint64_t segLo, uint64_t segHi, void* d_slab, uint64_t slabBytes,
+                       int primeSlab);
+    void* (*createStream)(int vendorIndex);
+    int (*destroyStream)(int vendorIndex, void* stream);
+    void* (*createEvent)(int vendorIndex);
+    int (*destroyEvent)(int vendorIndex, void* ev);
+    int (*recordEvent)(int vendorIndex, void* ev, void* stream);
+    int (*waitEvent)(int vendorIndex, void* ev, void* stream);
+    int (*syncEvent)(int vendorIndex, void* ev);
+    int (*elapsedEvents)(int vendorIndex, void* startEv, void* endEv, double* msOut);
+    int (*allocPinned)(int vendorIndex, void** h, uint64_t bytes);
+    int (*freePinned)(int vendorIndex, void* h);
+    int (*copyH2DAsync)(int vendorIndex, void* d_dst, const void* h_src, uint64_t bytes,
+                        void* stream);
+    int (*copyD2HAsync)(int vendorIndex, void* h_dst, const void* d_src, uint64_t bytes,
+                        void* stream);
+    int (*slabComputeAsync)(int vendorIndex, const uint32_t* h_primes, uint32_t numPrimes,
+                            uint64_t segLo, uint64_t segHi, void* d_slab, uint64_t slabBytes,
+                            void* computeStream, void* waitEvent);
+} SievePoolOps;
+
+/* source/sieve_slab_engine.cpp:450-457: the table when vendorIndex is a visible device. */
+const SievePoolOps* SievePoolGet_sm_100a(int vendorIndex);
+const SievePoolOps* SievePoolGet_sm_120(int vendorIndex);
+const SievePoolOps* SievePoolGet_gfx1201(int vendorIndex); /* always NULL */
+
+/* ---------------------------------------------------------------------------------- */
+/* M4 search (source/m4/gpu_search_kernel.cpp:31-66, gpu_search_launcher.h:43-50)      */
+/* ---------------------------------------------------------------------------------- */
+
+typedef int (*SearchKernelRunFn)(int deviceIndex, const uint8_t* d_primeMap,
+                                 uint64_t d_maxPrimeMapValue, uint64_t d_sumStart,
+                                 uint64_t d_sumLimit, uint32_t* d_pAtomicCount,
+                                 GpuRecord* d_pRecords);
+
+/* Evaluates the odd sums d_sumStart, d_sumStart+2, ... <= d_sumLimit (inclusive) against
+ * the map (values <= d_maxPrimeMapValue answered by the map, larger ones by Miller-Rabin)
+ * and writes each solution to slot (sum-d_sumStart)>>1 of d_pRecords, incrementing
+ * *d_pAtomicCount. The caller zero-fills (d_sumLimit-d_sumStart)/2+1 slots and the
+ * counter. Asynchronous on the legacy default stream (returns after the launch; a later
+ * synchronising copy completes it). d_sumStart must be odd (every reference caller passes
+ * sumStart|1). Replaces SearchKernelRun_<arch> (source/m4/gpu_search_kernel.cpp:31-51). */
+int SearchKernelRun_sm_100a(int deviceIndex, const uint8_t* d_primeMap,
+                            uint64_t d_maxPrimeMapValue, uint64_t d_sumStart,
+                            uint64_t d_sumLimit, uint32_t* d_pAtomicCount,
+                            GpuRecord* d_pRecords);
+/* source/m4/gpu_search_kernel.cpp:56-66 */
+SearchKernelRunFn SearchKernelGetLaunchFn_sm_100a(int deviceIndex);
+int SearchKernelRun_sm_120(int deviceIndex, const uint8_t* d_primeMap,
+                           uint64_t d_maxPrimeMapValue, uint64_t d_sumStart,
+                           uint64_t d_sumLimit, uint32_t* d_pAtomicCount,
+                           GpuRecord* d_pRecords);
+SearchKernelRunFn SearchKernelGetLaunchFn_sm_120(int deviceIndex);
+SearchKernelRunFn SearchKernelGetLaunchFn_gfx1201(int deviceIndex); /* always NULL */
+
+/* vendor "nvidia" launches SearchKernelRun_sm_100a; any other vendor returns -1 (the
+ * reference returns -1 when no launch function exists). Note the argument order
+ * (records before counter). Replaces GpuSearchLaunch (source/m4/gpu_search_launcher.cpp:36-61). */
+int GpuSearchLaunch(int deviceIndex, const char* vendor, const uint8_t* d_primeMap,
+                    uint64_t d_maxPrimeMapValue, uint64_t d_sumStart, uint64_t d_sumLimit,
+                    GpuRecord* d_pRecords, uint32_t* d_pAtomicCount);
+
+/* ---------------------------------------------------------------------------------- */
+/* Text output (source/m4/gpu_search_emission.cpp:34-96; reference/segmentedSieve.C:   */
+/* 645-677, 816-819). The C++ PrintOutputTags / FormatGpuSearchResult / GpuSearchEmit  */
+/* taking a GpuPrime are declared in gpu_prime.h.                                      */
+/* ---------------------------------------------------------------------------------- */
+
+/* One solution line (count field included, '\n'-terminated) into buf; returns its length
+ * or -1 when cap is too small. lowPrime/highPrime select the " (prime)" tags. */
+int ffb_format_line(uint32_t count, uint32_t sum, uint32_t low, uint32_t high, int lowPrime,
+                    int highPrime, char* buf, size_t cap);
+
+/* ---------------------------------------------------------------------------------- */
+/* Extensions (no reference counterpart): stream-aware device calls and the whole     */
+/* ff_sieve pipeline as one call.                                                      */
+/* ---------------------------------------------------------------------------------- */
+
+/* Geometry of `ff_sieve <sumStart> <sumLimit>` after the reference's argument handling
+ * (reference/segmentedSieve.C:844-879, Prime::Prime :136-182). nargs = number of
+ * positional arguments (0-2), a1/a2 their atoi() values. Writes the header lines into
+ * hdr (NUL-terminated) and returns their length; -1 on error or when the reference
+ * would stop with its "more memory" message (then hdr holds that message). */
+typedef struct {
+    uint32_t sumStart, sumLimit;
+    uint64_t maxPrimeMapValue;  /* mpv after the estimate and renormalisation branches */
+    uint64_t mapBytes;          /* (mpv+1+15)>>4 */
+    uint64_t numPrimesRequested;
+    uint64_t pmapSumLimit;      /* isqrt64((mpv-2)<<2)<<1 */
+} FfbGeometry;
+int ffb_geometry(int nargs, int32_t a1, int32_t a2, FfbGeometry* g, char* hdr, size_t cap);
+
+/* The sum sub-ranges ff_seg evaluates for [sumStart, sumLimit] in emission order
+ * (GenerateThreads' 62-way front/back partition, reference/segmentedSieve.C:706-792,
+ * applied once or twice per main's split at :905-912), threads = THREADS (31).
+ * Returns the number of ranges (firsts[i]..lasts[i], inclusive; odd sums from
+ * firsts[i]|1) or -1. */
+int ffb_schedule(uint32_t sumStart, uint32_t sumLimit, uint64_t maxPrimeMapValue,
+                 uint32_t threads, uint32_t* firsts, uint32_t* lasts, int cap);
+
+/* Full reference map for [0, maxPrimeMapValue] into d_map ((mpv+1+15)>>4 bytes rounded up
+ * to a multiple of 16, 16-byte aligned), stream-ordered on `stream` (a cudaStream_t; NULL = legacy default). */
+int ffb_sieve_map_async(int deviceIndex, uint64_t maxPrimeMapValue, uint8_t* d_map,
+                        void* stream);
+
+/* Packed search results for the odd sums lo..hi (lo, hi odd): d_rec[(s-lo)/2] = 0 or
+ * (low | lowPrime<<31) << 32 | (high | highPrime<<31). Values <= mapBound are answered by
+ * d_map, larger ones by Miller-Rabin. d_rec is zero-filled by the call. Stream-ordered. */
+int ffb_search_async(int deviceIndex, const uint8_t* d_map, uint64_t mapBound, uint32_t lo,
+                     uint32_t hi, uint64_t* d_rec, void* stream);
+
+/* Reads and clears the device error flags raised by kernels (1: Miller-Rabin outside the
+ * exact domain, 2: a divisor list overflowed, 4: bad launch input). Synchronises the
+ * device. Returns 0 and the flags in *flags. */
+int ffb_take_errors(int deviceIndex, uint32_t* flags);
+
+/* A resident context for repeated runs: device map grown to the largest limit asked for,
+ * record buffers and pinned staging. One context per thread at a time. */
+typedef struct FfbContext FfbContext;
+FfbContext* ffb_context_create(int deviceIndex);
+void ffb_context_destroy(FfbContext* ctx);
+
+/* The whole `ff_sieve` / ff_seg stdout for the given arguments (see ffb_geometry), with the
+ * timing lines in microseconds ("Prime time: <us> μs", "Freudenthal time: <us> μs").
+ * *text receives a malloc'd buffer (free with ffb_free), *len its length. ctx may be NULL
+ * (a temporary context is used). */
+int ffb_run(FfbContext* ctx, int nargs, int32_t a1, int32_t a2, char** text, size_t* len);
+void ffb_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FFB200_H */
