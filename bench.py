@@ -4,9 +4,10 @@ over the odd sums 5..2^21 (`ff_sieve 5 2097152`), byte-identical to the referenc
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-One step = the whole job for the range: the reference's full prime map (values up to
-274,877,906,959, 16 GiB) sieved on the device, then every odd sum of the range searched,
-leaving one packed record per sum in HBM. `value` is odd sums per second of that job on
+One step = the whole job for the range: the prime map sieved on the device (the reference's
+16 GiB map for values up to 274,877,906,959, extended to the 21.3 GiB that every probe of
+the search needs so that none falls back to Miller-Rabin), then every odd sum of the range
+searched, leaving one packed record per sum in HBM. `value` is odd sums per second of that job on
 device-resident data (CUDA events on the launching stream, max over ranks); `e2e` is the
 same metric through the public call a user makes (ffb_run: sieve, search, records copied
 to the host, the text emitted in ff_seg's order), timed on the host clock.
@@ -129,9 +130,11 @@ def ours(args, rank, world, dist):
     g = geometry_for(ffb, LIMIT)
     lo, hi = 5, LIMIT - 1                                  # odd sums of `ff_sieve 5 2097152`
     a, b = shard_bounds(lo, hi, world, rank)
-    # the map this shard's probes need: the reference's map for the shard's top sum
+    # the map this shard's probes need: the reference's map for the shard's top sum, or the
+    # larger bound under which every probe of the search is a map lookup (ffb_probe_bound;
+    # the output is the same either way, Miller-Rabin being exact)
     gs = geometry_for(ffb, b + 1)
-    mpv = gs.maxPrimeMapValue
+    mpv = max(gs.maxPrimeMapValue, lib.ffb_probe_bound(b))
     nsums = odd_sums(a, b)
     d_map = torch.empty(((mpv + 1 + 15) >> 4) + 64, dtype=torch.uint8, device="cuda")
     d_rec = torch.empty(max(nsums, 1), dtype=torch.int64, device="cuda")
@@ -152,6 +155,8 @@ def ours(args, rank, world, dist):
         step()
     torch.cuda.synchronize()
     assert ffb.take_errors(dev) == 0
+    stats = (ctypes.c_uint64 * 2)()
+    lib.ffb_search_stats(dev, stats, 1)
     evs = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
     t0 = torch.cuda.Event(enable_timing=True)
     t1 = torch.cuda.Event(enable_timing=True)
@@ -174,6 +179,9 @@ def ours(args, rank, world, dist):
     flags = ffb.take_errors(dev)
     if flags:
         raise RuntimeError(f"device error flags {flags:#x}")
+    lib.ffb_search_stats(dev, stats, 1)
+    probes_per_step = stats[0] // args.steps
+    stage2_per_step = stats[1] // args.steps
     # records of all shards to rank 0 (the exchange of the sharded job)
     if dist and world > 1:
         sizes = [odd_sums(*shard_bounds(lo, hi, world, r)) for r in range(world)]
@@ -191,7 +199,7 @@ def ours(args, rank, world, dist):
 
     # e2e through the public call (rank 0, the whole job on one GPU)
     e2e = None
-    if rank == 0:
+    if rank == 0 and not args.no_e2e:
         ctx = lib.ffb_context_create(dev)
         p, n = ctypes.c_void_p(), ctypes.c_size_t()
         for _ in range(max(1, args.warmup)):
@@ -227,13 +235,16 @@ def ours(args, rank, world, dist):
                 "algorithmic_bytes": map_bytes, "peak_source": peak_src,
                 "note": "algorithmic bytes = bitmap bytes written once"}
     else:
-        # search: random 32-byte sector probes of the map; algorithmic bytes per step =
-        # 32 B x the HBM-bound probes (2^k + o*b - 2 of the splits that pass the cheap test)
-        probes = SEARCH_DRAM_PROBES.get(LIMIT)
-        achieved = (32 * probes / (search_ms / 1e3) / 1e9) if probes else None
+        # search: each stage-1 probe (2^k + o*b - 2) reads one random 32-byte sector of the
+        # multi-GB map; the records are written once. Algorithmic bytes per step =
+        # 32 B x stage-1 probes + 8 B x sums (counted on the device in the timed steps).
+        alg = 32 * probes_per_step + 8 * nsums
+        achieved = alg / (search_ms / 1e3) / 1e9
         roof = {"kernel": "search_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak if achieved else None, "traffic": None,
-                "algorithmic_bytes": 32 * probes if probes else None, "peak_source": peak_src}
+                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
+                "algorithmic_bytes": alg, "stage1_probes": probes_per_step,
+                "stage2_items": stage2_per_step, "peak_source": peak_src,
+                "note": "latency-bound integer kernel; see profiles/ for pipe utilisation"}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args)
@@ -242,21 +253,17 @@ def ours(args, rank, world, dist):
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
             "scaling": "strong", "vs_baseline": None, "dtype": "u32/u64 integer", "data": "synthetic",
-            "config": {"workload": "ff_sieve 5 2097152: full reference map (16 GiB, mpv "
+            "config": {"workload": f"ff_sieve 5 {LIMIT}: prime map sieved on the device (values up "
+                                   f"to {mpv}, {map_bytes / 2**30:.1f} GiB; reference mpv "
                                    f"{g.maxPrimeMapValue}) + search of {job_sums} odd sums",
                        "sum_start": 5, "sum_limit": LIMIT, "map_bytes": map_bytes,
-                       "l2": "inputs larger than L2 (16 GiB map rewritten every step)",
+                       "l2": "inputs larger than L2 (the map is rewritten every step)",
                        "parallelism": f"sum shards x{world}" if world > 1 else "1 GPU"},
             "kernel_ms": {"sieve_tiles": sieve_ms, "search_kernel": search_ms},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             "gpu_launches": 2 * args.steps,
         }
         print(json.dumps(line), flush=True)
-
-
-# HBM-bound probes of the search at sumLimit 2^21 (search roofline);
-# filled in from the instrumented count when available.
-SEARCH_DRAM_PROBES = {}
 
 
 # ---------------------------------------------------------------------------------------
@@ -277,7 +284,7 @@ def ref_binary():
 # The sample: 8192 odd sums around 0.505 * 2^21, where the per-sum search cost equals the
 # average over 5..2^21 (the cumulative cost grows as ~s^2.05); ff_seg's own timers give its
 # sieve time for the sample's limit and its search time for the sample.
-SAMPLE = (1050625, 1067007)
+SAMPLE = (1073537, 1089919)
 
 
 def run_ff_seg(exe, lo, hi):
@@ -318,7 +325,8 @@ def cpu_baseline(args):
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                 "sample": "reference binary not built (oracle/_ref)"}
     v, info = ref_sample_value(exe, threads)
-    return {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+    return {"value": v, "unit": UNIT, "cores": min(threads, os.cpu_count() or threads),
+            "threads": threads, "host_cores": os.cpu_count(), "kind": "reference",
             "sample": f"ff_seg (THREADS={threads}) on odd sums {SAMPLE[0]}..{SAMPLE[1]} "
                       f"(8192 sums of average cost); its sieve time scaled to the 2^21 map and "
                       f"charged per sum", **info}
@@ -349,7 +357,8 @@ def reference_arm(args, rank):
         "dtype": "u32/u64 integer", "data": "synthetic",
         "config": {"workload": "ff_sieve 5 2097152 (bounded sample)", "sum_start": 5,
                    "sum_limit": LIMIT},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(threads, os.cpu_count() or threads),
+                         "threads": threads, "host_cores": os.cpu_count(), "kind": "reference",
                          "sample": f"ff_seg (THREADS={threads}, reference source) on odd sums "
                                    f"{SAMPLE[0]}..{SAMPLE[1]}; sieve time scaled to the 2^21 map "
                                    f"and charged per sum", "last": infos[-1]},
@@ -358,13 +367,18 @@ def reference_arm(args, rank):
 
 
 def main():
+    global LIMIT
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the public-call timing")
+    ap.add_argument("--limit", type=int, default=2097152,
+                    help="sumLimit of the job (2^21 for the reported line; smaller for profiling)")
     args = ap.parse_args()
+    LIMIT = args.limit
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

@@ -87,6 +87,11 @@ static uint32_t* sched_slot(DeviceState* s)
     return s->words + i;
 }
 static uint32_t* err_word(DeviceState* s) { return s->words + kSchedSlots; }
+// two 64-bit work counters of the search, 8-byte aligned after the error word
+static unsigned long long* stats_words(DeviceState* s)
+{
+    return reinterpret_cast<unsigned long long*>(s->words + kSchedSlots + 2);
+}
 
 // Search over odd sums lo..hi into packed records and/or GpuRecord slots.
 int run_search(int dev, const uint8_t* d_map, uint64_t bound, uint32_t lo, uint32_t hi,
@@ -116,6 +121,7 @@ int run_search(int dev, const uint8_t* d_map, uint64_t bound, uint32_t lo, uint3
     a.ntdiv = s->ntdiv;
     a.sched = sched_slot(s);
     a.err = err_word(s);
+    a.stats = stats_words(s);
     if (d_rec) FFB_CUDA(cudaMemsetAsync(d_rec, 0, 8ull * a.nsums, stream));
     FFB_CUDA(cudaMemsetAsync(a.sched, 0, 4, stream));
     return launch_search(a, s->sms, stream);
@@ -458,6 +464,25 @@ extern "C" int ffb_search_async(int deviceIndex, const uint8_t* d_map, uint64_t 
 {
     return run_search(deviceIndex, d_map, mapBound, lo, hi, d_rec, nullptr, 0, nullptr,
                       (cudaStream_t)stream);
+}
+
+extern "C" int ffb_search_stats(int deviceIndex, uint64_t* out, int reset)
+{
+    DeviceState* s = device_state(deviceIndex);
+    if (!s) return -1;
+    FFB_CUDA(cudaSetDevice(deviceIndex));
+    FFB_CUDA(cudaDeviceSynchronize());
+    FFB_CUDA(cudaMemcpy(out, stats_words(s), 16, cudaMemcpyDeviceToHost));
+    if (reset) FFB_CUDA(cudaMemset(stats_words(s), 0, 16));
+    return 0;
+}
+
+extern "C" uint64_t ffb_probe_bound(uint32_t maxSum)
+{
+    if (maxSum > kMaxSum) return 0;
+    const uint64_t s = maxSum;
+    const uint64_t v = s * s / 12 + s + 16;
+    return ((v >> 4) << 4) | 15;  // 16m-1: whole bytes of the map
 }
 
 extern "C" int ffb_take_errors(int deviceIndex, uint32_t* flags)

@@ -28,6 +28,7 @@ struct SearchArgs {
     uint32_t ntdiv;
     uint32_t* sched;        // [0]: next chunk of 32 sums (must be 0 at launch)
     uint32_t* err;          // error flags (ffb_device.cuh)
+    unsigned long long* stats;  // [0] stage-1 probes, [1] stage-2 items (or null)
 };
 
 // Packed per-sum record written by the search: 0 = no solution line, else

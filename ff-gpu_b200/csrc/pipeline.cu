@@ -1,5 +1,6 @@
 // pipeline.cu -- one `ff_sieve <sumStart> <sumLimit>` run as a library call (ffb_run):
-// the reference's full map sieved on the device, every sum of ff_seg's schedule searched
+// the prime map sieved on the device (the reference's, extended to every value the search
+// probes), every sum of ff_seg's schedule searched
 // on the device, the packed records copied back once, and the text emitted on the host
 // in ff_seg's order (reference/segmentedSieve.C:829-925).
 #include <cuda_runtime.h>
@@ -170,6 +171,12 @@ extern "C" int ffb_run(FfbContext* ctx, int nargs, int32_t a1, int32_t a2, char*
         std::fprintf(stderr, "ffb_run: sums above 2^25 are outside the exact domain\n");
         return -1;
     }
+    // The device map: the reference's (values up to mpv) or, when larger, one covering every
+    // value the search probes, so that no probe falls back to Miller-Rabin. IsPrime is exact
+    // either way, so the output does not depend on this choice.
+    uint64_t map_mpv = g.mpv;
+    if (lo <= hi) map_mpv = std::max(map_mpv, ffb_probe_bound(hi));
+    const uint64_t map_bytes = (map_mpv + 1 + 15) >> 4;
     FfbContext* c = ctx ? ctx : ffb_context_create(0);
     if (!c) return -1;
     int rc = 0;
@@ -177,14 +184,14 @@ extern "C" int ffb_run(FfbContext* ctx, int nargs, int32_t a1, int32_t a2, char*
     double prime_us = 0, freud_us = 0;
     do {
         const uint64_t nrec = lo <= hi ? ((uint64_t)hi - lo) / 2 + 1 : 1;
-        if ((rc = grow(c, g.map_bytes, nrec))) break;
+        if ((rc = grow(c, map_bytes, nrec))) break;
         cudaSetDevice(c->dev);
         const auto t0 = clk::now();
-        if ((rc = ffb_sieve_map_async(c->dev, g.mpv, c->d_map, c->stream))) break;
+        if ((rc = ffb_sieve_map_async(c->dev, map_mpv, c->d_map, c->stream))) break;
         if (cudaStreamSynchronize(c->stream) != cudaSuccess) { rc = -1; break; }
         const auto t1 = clk::now();
         if (lo <= hi) {
-            if ((rc = ffb_search_async(c->dev, c->d_map, g.mpv, lo, hi, c->d_rec, c->stream))) break;
+            if ((rc = ffb_search_async(c->dev, c->d_map, map_mpv, lo, hi, c->d_rec, c->stream))) break;
             if (cudaMemcpyAsync(c->h_rec, c->d_rec, 8 * nrec, cudaMemcpyDeviceToHost, c->stream) !=
                     cudaSuccess ||
                 cudaStreamSynchronize(c->stream) != cudaSuccess) {

@@ -218,6 +218,7 @@ __device__ void drain_a(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
     const uint32_t take = st.na < 32 ? st.na : 32;
     const uint32_t base = st.na - take;
     const bool act = (uint32_t)lane < take;
+    if (lane == 0 && A.stats) atomicAdd(&A.stats[0], (unsigned long long)take);
     const uint32_t item = act ? Q.a[base + lane] : 0;
     __syncwarp();
     st.na = base;
@@ -231,6 +232,7 @@ __device__ void drain_b(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
     const uint32_t take = st.nb < 32 ? st.nb : 32;
     const uint32_t base = st.nb - take;
     const bool act = (uint32_t)lane < take;
+    if (lane == 0 && A.stats) atomicAdd(&A.stats[1], (unsigned long long)take);
     const uint32_t item = act ? Q.b[base + lane] : 0;
     __syncwarp();
     st.nb = base;

@@ -8,8 +8,9 @@
 //
 // Fast path (the list starts with the odd primes 3,5,7,... in order):
 //   * The slab is cut into shared-memory tiles; a persistent grid walks the tiles.
-//   * Each tile starts from a pre-computed wheel pattern for 3,5,7,11,13 (period 15015 odd
-//     numbers) read with funnel shifts, so those primes are never marked one by one.
+//   * Each tile starts from three pre-computed patterns (the odd numbers free of 3..13, of
+//     17,19,23 and of 29,31,37; periods 15015, 7429 and 33263 odd numbers) read with funnel
+//     shifts and ANDed, so the eleven smallest odd primes are never marked one by one.
 //   * Primes with many marks per tile are marked warp-cooperatively (each lane a strided
 //     subset of the multiples), the rest one prime per thread; all with shared-memory
 //     atomicAnd. The first multiple in a tile comes from a Barrett reduction.
@@ -27,11 +28,19 @@ namespace ffb {
 namespace {
 
 constexpr int kSieveThreads = 512;
-constexpr uint32_t kWheelPeriod = 15015;                      // 3*5*7*11*13 odd numbers
-constexpr uint32_t kWheelWords = (kWheelPeriod + 63) / 32 + 1;
 
-// Wheel bit j (LSB-first) = 1 iff the odd number 2j+1 has no factor in {3,5,7,11,13};
-// the table is extended past the period so any 32-bit window can be read unwrapped.
+// Pre-sieve patterns: bit j (LSB-first) of pattern t is 1 iff the odd number 2j+1 has no
+// factor among the primes of group t; each pattern repeats with the product of its
+// primes (in odd numbers) and is stored with one extra period word so any 32-bit window
+// can be read without wrapping.
+constexpr uint32_t kPeriod0 = 3 * 5 * 7 * 11 * 13;   // 15015
+constexpr uint32_t kPeriod1 = 17 * 19 * 23;          // 7429
+constexpr uint32_t kPeriod2 = 29 * 31 * 37;          // 33263
+constexpr uint32_t kWords0 = (kPeriod0 + 63) / 32 + 1;
+constexpr uint32_t kWords1 = (kPeriod1 + 63) / 32 + 1;
+constexpr uint32_t kWords2 = (kPeriod2 + 63) / 32 + 1;
+constexpr uint32_t kWheelWords = kWords0 + kWords1 + kWords2;
+constexpr int kWheelPrimes = 11;                     // 3 .. 37
 __device__ uint32_t g_wheel[kWheelWords];
 
 struct TileArgs {
@@ -41,7 +50,7 @@ struct TileArgs {
     uint64_t nbits;         // bits of odd values < seg_hi
     uint64_t total_bits;    // 8 * out_bytes
     const uint32_t* primes; // device list (standard prefix)
-    const uint64_t* mu;     // floor(2^64 / p) per prime
+    const uint64_t* mu;     // floor((2^64-1) / p) per prime
     uint32_t ibeg, ismall, iend;  // [ibeg, ismall): warp-cooperative, [ismall, iend): per thread
     int wheel;
     int clear_one;          // clear the bit of the value 1 (seg_lo == 0)
@@ -71,6 +80,12 @@ __device__ __forceinline__ uint64_t first_bit(uint64_t m_lo, uint64_t base_odd, 
     return (f - base_odd) >> 1;
 }
 
+__device__ __forceinline__ uint32_t window(const uint32_t* w, uint64_t j, uint32_t period)
+{
+    const uint32_t ph = (uint32_t)(j % period);
+    return __funnelshift_r(w[ph >> 5], w[(ph >> 5) + 1], ph & 31);
+}
+
 __global__ void __launch_bounds__(kSieveThreads) sieve_tiles(const TileArgs A)
 {
     extern __shared__ uint32_t smem[];
@@ -80,21 +95,20 @@ __global__ void __launch_bounds__(kSieveThreads) sieve_tiles(const TileArgs A)
         for (uint32_t i = threadIdx.x; i < kWheelWords; i += blockDim.x) wheel[i] = g_wheel[i];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const uint64_t tile_bits = (uint64_t)A.tile_words * 32;
-    const uint64_t j0 = (A.base_odd - 1) >> 1;  // wheel index of bit 0
+    const uint64_t j0 = (A.base_odd - 1) >> 1;  // pattern index of bit 0
 
     for (uint64_t t = blockIdx.x; t < A.ntiles; t += gridDim.x) {
         const uint64_t m0 = t * tile_bits;
         const uint64_t m1 = min(m0 + tile_bits, A.total_bits);
         const uint32_t words = (uint32_t)((m1 - m0 + 31) >> 5);
-        __syncthreads();  // previous tile fully stored; wheel loaded
+        __syncthreads();  // previous tile fully stored; patterns loaded
         // ---- 1. initial pattern ----
         for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
             const uint64_t gm = m0 + 32ull * w;
             uint32_t x = 0xFFFFFFFFu;
             if (A.wheel) {
-                const uint32_t ph = (uint32_t)((j0 + gm) % kWheelPeriod);
-                const uint32_t lo = wheel[ph >> 5], hi = wheel[(ph >> 5) + 1];
-                x = __funnelshift_r(lo, hi, ph & 31);
+                x = window(wheel, j0 + gm, kPeriod0) & window(wheel + kWords0, j0 + gm, kPeriod1) &
+                    window(wheel + kWords0 + kWords1, j0 + gm, kPeriod2);
             }
             if (gm + 32 > A.nbits) {  // bits of values >= seg_hi stay set
                 const uint64_t keep = A.nbits > gm ? A.nbits - gm : 0;
@@ -104,30 +118,33 @@ __global__ void __launch_bounds__(kSieveThreads) sieve_tiles(const TileArgs A)
         }
         __syncthreads();
         const uint64_t mlim = min(m1, A.nbits);
+        const uint32_t rl = (uint32_t)(mlim > m0 ? mlim - m0 : 0);  // tile-relative limit
         // ---- 2a. primes with many multiples per tile: one warp per prime ----
         for (uint32_t i = A.ibeg + warp; i < A.ismall; i += nwarps) {
             const uint64_t p = A.primes[i];
-            uint64_t m = first_bit(m0, A.base_odd, p, A.mu[i]) + lane * p;
-            const uint64_t step = 32 * p;
-            for (; m < mlim; m += step) {
-                const uint32_t r = (uint32_t)(m - m0);
-                atomicAnd(&tile[r >> 5], ~(1u << (r & 31)));
-            }
+            const uint64_t f = first_bit(m0, A.base_odd, p, A.mu[i]);
+            if (f >= mlim) continue;
+            const uint32_t p32 = (uint32_t)p, step = 32 * p32;
+            uint32_t r = (uint32_t)(f - m0) + lane * p32;
+#pragma unroll 4
+            for (; r < rl; r += step) atomicAnd(&tile[r >> 5], ~(1u << (r & 31)));
         }
         // ---- 2b. the rest: one thread per prime ----
         for (uint32_t i = A.ismall + threadIdx.x; i < A.iend; i += blockDim.x) {
             const uint64_t p = A.primes[i];
-            for (uint64_t m = first_bit(m0, A.base_odd, p, A.mu[i]); m < mlim; m += p) {
-                const uint32_t r = (uint32_t)(m - m0);
+            const uint64_t f = first_bit(m0, A.base_odd, p, A.mu[i]);
+            if (f >= mlim) continue;
+            const uint32_t p32 = (uint32_t)p;
+#pragma unroll 4
+            for (uint32_t r = (uint32_t)(f - m0); r < rl; r += p32)
                 atomicAnd(&tile[r >> 5], ~(1u << (r & 31)));
-            }
         }
         __syncthreads();
-        // ---- 3. the wheel primes themselves and the value 1 ----
-        if (threadIdx.x == 0 && A.base_odd <= 13) {
-            const uint32_t wp[5] = {3, 5, 7, 11, 13};
+        // ---- 3. the pattern primes themselves and the value 1 ----
+        if (threadIdx.x == 0 && A.base_odd <= 37) {
+            const uint32_t wp[kWheelPrimes] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
             if (A.wheel)
-                for (int q = 0; q < 5; ++q) {
+                for (int q = 0; q < kWheelPrimes; ++q) {
                     if (wp[q] < A.base_odd) continue;
                     const uint64_t m = (wp[q] - A.base_odd) >> 1;
                     if (m >= m0 && m < mlim) tile[(m - m0) >> 5] |= 1u << ((m - m0) & 31);
@@ -177,9 +194,18 @@ int upload_wheel()
     FFB_CUDA(cudaGetDevice(&dev));
     if (done_dev == dev) return 0;
     std::vector<uint32_t> w(kWheelWords, 0);
-    for (uint32_t j = 0; j < kWheelWords * 32; ++j) {
-        const uint32_t v = 2 * (j % kWheelPeriod) + 1;
-        if (v % 3 && v % 5 && v % 7 && v % 11 && v % 13) w[j >> 5] |= 1u << (j & 31);
+    const uint32_t periods[3] = {kPeriod0, kPeriod1, kPeriod2};
+    const uint32_t words[3] = {kWords0, kWords1, kWords2};
+    const uint32_t group[3][5] = {{3, 5, 7, 11, 13}, {17, 19, 23, 0, 0}, {29, 31, 37, 0, 0}};
+    uint32_t off = 0;
+    for (int g = 0; g < 3; ++g) {
+        for (uint32_t j = 0; j < words[g] * 32; ++j) {
+            const uint32_t v = 2 * (j % periods[g]) + 1;
+            bool keep = true;
+            for (int q = 0; q < 5 && group[g][q]; ++q) keep = keep && v % group[g][q] != 0;
+            if (keep) w[off + (j >> 5)] |= 1u << (j & 31);
+        }
+        off += words[g];
     }
     FFB_CUDA(cudaMemcpyToSymbol(g_wheel, w.data(), w.size() * 4));
     done_dev = dev;
@@ -234,7 +260,7 @@ int launch_sieve(const SieveArgs& a, int sms, cudaStream_t stream)
     // primes of the standard prefix with p*p < seg_hi mark something
     uint32_t iend = 0;
     while (iend < std_n && (uint64_t)h[off + iend] * h[off + iend] < a.seg_hi) ++iend;
-    const int wheel = std_n >= 5 && iend >= 1;  // wheel needs 3..13 in the list
+    const int wheel = std_n >= kWheelPrimes;  // the patterns need 3..37 in the list
     // Barrett constants for the prefix
     std::vector<uint64_t> mu(iend ? iend : 1);
     for (uint32_t i = 0; i < iend; ++i) mu[i] = ~0ull / h[off + i];
@@ -257,7 +283,7 @@ int launch_sieve(const SieveArgs& a, int sms, cudaStream_t stream)
     T.mu = d_mu;
     T.wheel = wheel;
     T.clear_one = a.clear_one && a.seg_lo == 0;
-    T.ibeg = wheel ? 5 : 0;
+    T.ibeg = wheel ? kWheelPrimes : 0;
     if (T.ibeg > iend) T.ibeg = iend;
     uint32_t tile_bytes = a.tile_bytes ? a.tile_bytes : 96 * 1024;
     tile_bytes = (tile_bytes + 15) & ~15u;

@@ -200,6 +200,17 @@ int ffb_sieve_map_async(int deviceIndex, uint64_t maxPrimeMapValue, uint8_t* d_m
 int ffb_search_async(int deviceIndex, const uint8_t* d_map, uint64_t mapBound, uint32_t lo,
                      uint32_t hi, uint64_t* d_rec, void* stream);
 
+/* Work done by the searches on a device since the last reset: out[0] = probes of
+ * 2^k + o*b - 2 (one random map sector each), out[1] = AllButOne... evaluations.
+ * Synchronises the device; reset != 0 clears the counters. */
+int ffb_search_stats(int deviceIndex, uint64_t* out, int reset);
+
+/* The smallest map bound (of the form 16m-1) at or above every value the search probes for
+ * sums up to maxSum: the pair sums it tests are at most maxSum^2/12 + maxSum (the divisor 3
+ * of a product below maxSum^2/4, or the even-phase pair with odd part 3), so with a map up
+ * to this bound no probe needs Miller-Rabin. Returns 0 above the supported domain. */
+uint64_t ffb_probe_bound(uint32_t maxSum);
+
 /* Reads and clears the device error flags raised by kernels (1: Miller-Rabin outside the
  * exact domain, 2: a divisor list overflowed, 4: bad launch input). Synchronises the
  * device. Returns 0 and the flags in *flags. */
