@@ -73,6 +73,9 @@ SIGNATURES = {
     "ffb_take_errors": (ctypes.c_int, [ctypes.c_int, u32p]),
     "ffb_probe_bound": (ctypes.c_uint64, [ctypes.c_uint32]),
     "ffb_search_stats": (ctypes.c_int, [ctypes.c_int, u64p, ctypes.c_int]),
+    "ffb_search_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                                          ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p]),
     "ffb_context_create": (ctypes.c_void_p, [ctypes.c_int]),
     "ffb_context_destroy": (None, [ctypes.c_void_p]),
     "ffb_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,

@@ -211,6 +211,26 @@ int ffb_search_stats(int deviceIndex, uint64_t* out, int reset);
  * to this bound no probe needs Miller-Rabin. Returns 0 above the supported domain. */
 uint64_t ffb_probe_bound(uint32_t maxSum);
 
+/* The search of ffb_search_async without any device allocation. No counterpart in the
+ * reference. For callers that cannot call cudaMalloc: a host whose device memory is owned by
+ * its own pool or framework allocator (memory reserved up front, outside allocations
+ * forbidden or accounted as failures), or a latency-critical caller for which an allocation
+ * or a free may synchronise the device. Every value here lives in a fixed 104,912-byte array
+ * compiled into the library (work counter, error word, the table of odd primes below 2^16),
+ * which each GPU that loads the library holds until the process exits.
+ *   - Same inputs and output as ffb_search_async: odd sums lo..hi (lo odd, hi <= 2^25; other
+ *     ranges are rejected with -1 and a message), d_map/mapBound, d_rec zero-filled by the
+ *     call. d_err (optional, device) receives the error flags of ffb_take_errors; NULL keeps
+ *     them in the library's array.
+ *   - The first call on a device sets the array up (its device address, the prime table
+ *     copied in, synchronously) with that device current; make that first call before any
+ *     stream capture.
+ *   - Calls share the one array; it keeps the last call's contents, and the call clears the
+ *     counter it needs. Calls that overlap on the GPU (different streams, same device) race
+ *     on it: serialise them. */
+int ffb_search_noalloc(int deviceIndex, const uint8_t* d_map, uint64_t mapBound, uint32_t lo,
+                       uint32_t hi, uint64_t* d_rec, uint32_t* d_err, void* stream);
+
 /* Reads and clears the device error flags raised by kernels (1: Miller-Rabin outside the
  * exact domain, 2: a divisor list overflowed, 4: bad launch input). Synchronises the
  * device. Returns 0 and the flags in *flags. */
