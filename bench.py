@@ -248,6 +248,9 @@ def ours(args, rank, world, dist):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(args)
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched and LIMIT == 2097152:
+        batched = batched_section(args, dev)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -261,9 +264,69 @@ def ours(args, rank, world, dist):
                        "parallelism": f"sum shards x{world}" if world > 1 else "1 GPU"},
             "kernel_ms": {"sieve_tiles": sieve_ms, "search_kernel": search_ms},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "batched": batched,
             "gpu_launches": 2 * args.steps,
         }
         print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------------------
+# batched mode: 256 ranges (seed 0) against the plain method once per range
+# ---------------------------------------------------------------------------------------
+def range_sums(a, b):
+    s = max(a | 1, 5)
+    return (b - s) // 2 + 1 if b >= s else 0
+
+
+def batched_section(args, dev):
+    import ffb200 as ffb
+    import workloads
+    lib = ffb.load()
+    ranges = workloads.batched_ranges(seed=0)
+    sums = sum(range_sums(a, b) for a, b in ranges)
+    t0 = time.perf_counter()
+    batch = ffb.Batch(ranges, dev=dev, autotune=True)
+    setup_s = time.perf_counter() - t0
+    try:
+        for _ in range(max(1, args.warmup)):
+            batch.run()
+        times, dev_ms = [], []
+        for _ in range(args.steps):
+            s = time.perf_counter()
+            batch.run()
+            times.append(time.perf_counter() - s)
+            info = batch.info()
+            dev_ms.append(info["sieveMs"] + info["searchMs"])
+        info = batch.info()
+    finally:
+        batch.close()
+    # the plain method, one ffb_run per range, on an evenly spaced sample of the ranges
+    ctx = lib.ffb_context_create(dev)
+    sample = ranges[::16]
+    p, n = ctypes.c_void_p(), ctypes.c_size_t()
+    plain_t, plain_sums = 0.0, 0
+    try:
+        assert lib.ffb_run(ctx, 2, sample[0][0], sample[0][1], ctypes.byref(p), ctypes.byref(n)) == 0
+        lib.ffb_free(p)
+        for a, b in sample:
+            s = time.perf_counter()
+            assert lib.ffb_run(ctx, 2, a, b, ctypes.byref(p), ctypes.byref(n)) == 0
+            plain_t += time.perf_counter() - s
+            lib.ffb_free(p)
+            plain_sums += range_sums(a, b)
+    finally:
+        lib.ffb_context_destroy(ctx)
+    value = sums / statistics.mean(times)
+    plain = plain_sums / plain_t
+    return {"workload": "256 ranges from seed 0 (start U{5..2^21}, length floor(2^U[8,18]))",
+            "value": value, "unit": UNIT, "ms_per_batch": 1e3 * statistics.mean(times),
+            "device_ms_per_batch": statistics.mean(dev_ms), "sums_per_batch": sums,
+            "distinct_sums": info["sums"], "intervals": info["intervals"],
+            "map_bytes": info["mapBytes"], "sieve_tile_bytes": info["sieveTileBytes"],
+            "search_warps": info["searchWarps"], "setup_s_incl_autotune": setup_s,
+            "plain_one_launch_per_range": {"value": plain, "unit": UNIT,
+                                           "sample": f"{len(sample)} of the 256 ranges (every 16th)"},
+            "vs_plain": value / plain}
 
 
 # ---------------------------------------------------------------------------------------
@@ -375,6 +438,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the public-call timing")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-mode section")
     ap.add_argument("--limit", type=int, default=2097152,
                     help="sumLimit of the job (2^21 for the reported line; smaller for profiling)")
     args = ap.parse_args()

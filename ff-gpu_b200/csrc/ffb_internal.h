@@ -29,6 +29,11 @@ struct SearchArgs {
     uint32_t* sched;        // [0]: next chunk of 32 sums (must be 0 at launch)
     uint32_t* err;          // error flags (ffb_device.cuh)
     unsigned long long* stats;  // [0] stage-1 probes, [1] stage-2 items (or null)
+    const uint4* seg = nullptr;  // work queue of disjoint intervals {lo, count, record base, first
+                            // chunk}, largest sums first (or null: the single range lo..hi)
+    uint32_t nseg = 0;      // intervals in seg (0: single range)
+    uint32_t nchunks = 0;   // chunks of 32 sums over all intervals
+    uint32_t warps = 0;     // warps per block: 4, 8 or 16 (0: 8)
 };
 
 // Packed per-sum record written by the search: 0 = no solution line, else
@@ -61,6 +66,13 @@ struct SieveArgs {
 };
 
 int launch_sieve(const SieveArgs& a, int sms, cudaStream_t stream);
+
+// A sieve analysed once (device tables allocated and uploaded); enqueue_sieve_plan launches
+// only kernels, so it can be captured into a CUDA graph and replayed.
+struct SievePlan;
+SievePlan* create_sieve_plan(const SieveArgs& a, int sms);
+int enqueue_sieve_plan(const SievePlan* p, cudaStream_t stream);
+void destroy_sieve_plan(SievePlan* p);
 int launch_search(const SearchArgs& a, int sms, cudaStream_t stream);
 
 // Entry helpers shared by the C ABI and the pipeline (capi.cu).

@@ -26,7 +26,6 @@
 namespace ffb {
 namespace {
 
-constexpr int kWarps = 8;        // warps per block
 constexpr int kQueue = 64;       // per-warp queue capacity (entries)
 constexpr int kMaxPf = 16;       // distinct odd prime factors of a product < 2^52
 constexpr int kMaxDiv = 64;      // divisor list of one AllButOne... call
@@ -296,13 +295,13 @@ __device__ bool run_phase(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
     return true;
 }
 
-__device__ void write_result(const SearchArgs& A, uint32_t s, uint32_t ta, uint32_t tb)
+__device__ void write_result(const SearchArgs& A, uint32_t s, uint32_t ri, uint32_t ta, uint32_t tb)
 {
     uint32_t lo = ta < tb ? ta : tb, hi = ta < tb ? tb : ta;
     if (A.rec) {
         const bool lp = is_prime(A.map, A.bound, lo, A.err);
         const bool hp = is_prime(A.map, A.bound, hi, A.err);
-        A.rec[(s - A.lo) >> 1] = ((uint64_t)(lo | (lp ? 0x80000000u : 0u)) << 32) |
+        A.rec[ri] = ((uint64_t)(lo | (lp ? 0x80000000u : 0u)) << 32) |
                                  (uint64_t)(hi | (hp ? 0x80000000u : 0u));
     }
     if (A.grec) {
@@ -316,12 +315,13 @@ __device__ void write_result(const SearchArgs& A, uint32_t s, uint32_t ta, uint3
     }
 }
 
-__global__ void __launch_bounds__(kWarps * 32) search_kernel(const SearchArgs A)
+template <int W>
+__global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
 {
-    __shared__ WarpQ queues[kWarps];
+    __shared__ WarpQ queues[W];
     const int lane = threadIdx.x & 31;
     WarpQ& Q = queues[threadIdx.x >> 5];
-    const uint32_t nchunks = (A.nsums + 31) / 32;
+    const uint32_t nchunks = A.nseg ? A.nchunks : (A.nsums + 31) / 32;
     for (;;) {
         uint32_t c = 0;
         if (lane == 0) c = atomicAdd(A.sched, 1u);
@@ -329,9 +329,31 @@ __global__ void __launch_bounds__(kWarps * 32) search_kernel(const SearchArgs A)
         if (c >= nchunks) break;
 
         // ---- lane-parallel: filter + Power2Prime for 32 sums (largest first) ----
-        const uint32_t idx = c * 32 + lane;
-        const bool act = idx < A.nsums;
-        const uint32_t s = act ? A.hi - 2 * idx : 5;
+        bool act;
+        uint32_t s = 5, ri = 0;
+        if (A.nseg == 0) {
+            const uint32_t idx = c * 32 + lane;
+            act = idx < A.nsums;
+            if (act) {
+                s = A.hi - 2 * idx;
+                ri = (s - A.lo) >> 1;
+            }
+        } else {
+            // work queue of disjoint sum intervals, largest first: the interval whose chunks
+            // contain chunk c (entries {lo, count, record base, first chunk}, ascending in .w)
+            uint32_t a = 0, b = A.nseg - 1;
+            while (a < b) {
+                const uint32_t m = (a + b + 1) >> 1;
+                if (__ldg(&A.seg[m].w) <= c) a = m; else b = m - 1;
+            }
+            const uint4 g = __ldg(&A.seg[a]);
+            const uint32_t idx = (c - g.w) * 32 + lane;
+            act = idx < g.y;
+            if (act) {
+                s = g.x + 2 * (g.y - 1 - idx);  // descending within the interval
+                ri = g.z + ((s - g.x) >> 1);
+            }
+        }
         bool surv = false;
         uint32_t cnt = 0, ta = 0, tb = 0, comp = 0;
         if (act) {
@@ -361,6 +383,7 @@ __global__ void __launch_bounds__(kWarps * 32) search_kernel(const SearchArgs A)
             smask &= smask - 1;
             SumState st;
             st.s = __shfl_sync(0xFFFFFFFFu, s, src);
+            const uint32_t sri = __shfl_sync(0xFFFFFFFFu, ri, src);
             st.count = __shfl_sync(0xFFFFFFFFu, cnt, src);
             st.ta = __shfl_sync(0xFFFFFFFFu, ta, src);
             st.tb = __shfl_sync(0xFFFFFFFFu, tb, src);
@@ -381,7 +404,7 @@ __global__ void __launch_bounds__(kWarps * 32) search_kernel(const SearchArgs A)
                 drain_b(st, Q, A, lane);
                 open = st.count <= 1;
             }
-            if (open && st.count == 1 && lane == 0) write_result(A, st.s, st.ta, st.tb);
+            if (open && st.count == 1 && lane == 0) write_result(A, st.s, sri, st.ta, st.tb);
             __syncwarp();
         }
     }
@@ -389,19 +412,30 @@ __global__ void __launch_bounds__(kWarps * 32) search_kernel(const SearchArgs A)
 
 }  // namespace
 
-int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
+template <int W>
+int launch_w(const SearchArgs& a, int sms, cudaStream_t stream)
 {
-    if (a.nsums == 0) return 0;
     int per_sm = 0;
-    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel, kWarps * 32, 0));
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel<W>, W * 32, 0));
     if (per_sm < 1) per_sm = 1;
-    uint32_t chunks = (a.nsums + 31) / 32;
+    const uint32_t chunks = a.nseg ? a.nchunks : (a.nsums + 31) / 32;
     uint32_t blocks = (uint32_t)sms * (uint32_t)per_sm;
-    const uint32_t need = (chunks + kWarps - 1) / kWarps;
+    const uint32_t need = (chunks + W - 1) / W;
     if (blocks > need) blocks = need;
-    search_kernel<<<blocks, kWarps * 32, 0, stream>>>(a);
+    if (blocks == 0) return 0;
+    search_kernel<W><<<blocks, W * 32, 0, stream>>>(a);
     FFB_CUDA(cudaGetLastError());
     return 0;
+}
+
+int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
+{
+    if (a.nseg == 0 && a.nsums == 0) return 0;
+    switch (a.warps) {
+    case 4: return launch_w<4>(a, sms, stream);
+    case 16: return launch_w<16>(a, sms, stream);
+    default: return launch_w<8>(a, sms, stream);
+    }
 }
 
 }  // namespace ffb

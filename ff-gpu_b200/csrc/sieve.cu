@@ -232,11 +232,29 @@ void host_odd_primes(uint64_t limit, uint32_t** out, uint32_t* n)
     std::copy(v.begin(), v.end(), *out);
 }
 
+// Host-side analysis of one sieve request: the tiled kernel's arguments (device table
+// pointers filled in by the caller), its launch shape, the table contents, and the list
+// entries that go through sieve_generic.
+struct SieveHost {
+    TileArgs T;
+    size_t smem = 0;
+    unsigned blocks = 0;
+    bool tiles = false;
+    std::vector<uint64_t> mu;
+    std::vector<uint32_t> list;
+    struct Gen {
+        uint64_t p, first, nmarks;
+        unsigned grid;
+    };
+    std::vector<Gen> gen;
+};
+
+namespace {
+
 // The standard prefix of the list goes through the tiled kernel; every other entry through
 // sieve_generic. Marks only ever clear bits, so splitting the list is exact.
-int launch_sieve(const SieveArgs& a, int sms, cudaStream_t stream)
+int analyse(const SieveArgs& a, int sms, SieveHost& H)
 {
-    if (a.seg_hi <= a.seg_lo) return 0;
     if (upload_wheel()) return -1;
     const uint64_t out_bytes = (a.seg_hi - a.seg_lo + 15) >> 4;
     if (((uintptr_t)a.out & 15) != 0) {
@@ -261,26 +279,18 @@ int launch_sieve(const SieveArgs& a, int sms, cudaStream_t stream)
     uint32_t iend = 0;
     while (iend < std_n && (uint64_t)h[off + iend] * h[off + iend] < a.seg_hi) ++iend;
     const int wheel = std_n >= kWheelPrimes;  // the patterns need 3..37 in the list
-    // Barrett constants for the prefix
-    std::vector<uint64_t> mu(iend ? iend : 1);
-    for (uint32_t i = 0; i < iend; ++i) mu[i] = ~0ull / h[off + i];
-    // device copy of the marked prefix and its Barrett constants (stream-ordered scratch)
-    const size_t nl = iend ? iend : 1;
-    uint8_t* scratch = nullptr;
-    FFB_CUDA(cudaMallocAsync((void**)&scratch, 12 * nl + 16, stream));
-    uint64_t* d_mu = (uint64_t*)scratch;
-    uint32_t* d_list = (uint32_t*)(scratch + 8 * nl);
-    FFB_CUDA(cudaMemcpyAsync(d_mu, mu.data(), 8 * nl, cudaMemcpyHostToDevice, stream));
-    if (iend) FFB_CUDA(cudaMemcpyAsync(d_list, h + off, 4ull * iend, cudaMemcpyHostToDevice, stream));
+    H.list.assign(h + off, h + off + iend);
+    H.mu.resize(iend);
+    for (uint32_t i = 0; i < iend; ++i) H.mu[i] = ~0ull / h[off + i];   // Barrett constants
 
-    TileArgs T;
+    TileArgs& T = H.T;
     T.out = a.out;
     T.out_bytes = out_bytes;
     T.base_odd = a.seg_lo | 1;
     T.nbits = a.seg_hi > T.base_odd ? (a.seg_hi - T.base_odd + 1) / 2 : 0;
     T.total_bits = out_bytes * 8;
-    T.primes = d_list;
-    T.mu = d_mu;
+    T.primes = nullptr;
+    T.mu = nullptr;
     T.wheel = wheel;
     T.clear_one = a.clear_one && a.seg_lo == 0;
     T.ibeg = wheel ? kWheelPrimes : 0;
@@ -293,20 +303,18 @@ int launch_sieve(const SieveArgs& a, int sms, cudaStream_t stream)
     while (T.ismall < iend && (uint64_t)h[off + T.ismall] * 32 < tile_bits) ++T.ismall;
     T.iend = iend;
     T.ntiles = (T.total_bits + tile_bits - 1) / tile_bits;
-    const size_t smem = 4ull * (T.tile_words + kWheelWords);
-    FFB_CUDA(cudaFuncSetAttribute(sieve_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    H.smem = 4ull * (T.tile_words + kWheelWords);
+    FFB_CUDA(cudaFuncSetAttribute(sieve_tiles, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)H.smem));
     int per_sm = 0;
-    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sieve_tiles, kSieveThreads, smem));
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sieve_tiles, kSieveThreads, H.smem));
     if (per_sm < 1) {
         std::fprintf(stderr, "ffb: sieve tile of %u bytes does not fit on an SM\n", tile_bytes);
-        cudaFreeAsync(scratch, stream);
         return -1;
     }
     uint64_t blocks = (uint64_t)sms * per_sm;
     if (blocks > T.ntiles) blocks = T.ntiles;
-    sieve_tiles<<<(unsigned)blocks, kSieveThreads, smem, stream>>>(T);
-    FFB_CUDA(cudaGetLastError());
-    FFB_CUDA(cudaFreeAsync(scratch, stream));
+    H.blocks = (unsigned)blocks;
+    H.tiles = T.ntiles > 0;
 
     // every entry outside the standard prefix, literally
     for (uint32_t i = 0; i < a.nprimes; ++i) {
@@ -322,11 +330,97 @@ int launch_sieve(const SieveArgs& a, int sms, cudaStream_t stream)
         const uint64_t nmarks = (a.seg_hi - first + 2 * p - 1) / (2 * p);
         uint64_t g = (nmarks + 255) / 256;
         if (g > (uint64_t)sms * 16) g = (uint64_t)sms * 16;
-        sieve_generic<<<(unsigned)g, 256, 0, stream>>>((uint32_t*)a.out, a.seg_lo, a.seg_hi, p,
-                                                       first, nmarks);
+        H.gen.push_back({p, first, nmarks, (unsigned)g});
+    }
+    return 0;
+}
+
+int enqueue(const SieveHost& H, const SieveArgs& a, cudaStream_t stream)
+{
+    if (H.tiles) {
+        sieve_tiles<<<H.blocks, kSieveThreads, H.smem, stream>>>(H.T);
+        FFB_CUDA(cudaGetLastError());
+    }
+    for (const SieveHost::Gen& g : H.gen) {
+        sieve_generic<<<g.grid, 256, 0, stream>>>((uint32_t*)a.out, a.seg_lo, a.seg_hi, g.p,
+                                                  g.first, g.nmarks);
         FFB_CUDA(cudaGetLastError());
     }
     return 0;
+}
+
+}  // namespace
+
+int launch_sieve(const SieveArgs& a, int sms, cudaStream_t stream)
+{
+    if (a.seg_hi <= a.seg_lo) return 0;
+    SieveHost H;
+    if (analyse(a, sms, H)) return -1;
+    // device copy of the marked prefix and its Barrett constants (stream-ordered scratch)
+    const size_t nl = H.list.empty() ? 1 : H.list.size();
+    uint8_t* scratch = nullptr;
+    FFB_CUDA(cudaMallocAsync((void**)&scratch, 12 * nl + 16, stream));
+    H.T.mu = (const uint64_t*)scratch;
+    H.T.primes = (const uint32_t*)(scratch + 8 * nl);
+    int rc = 0;
+    if (!H.list.empty() &&
+        (cudaMemcpyAsync(scratch, H.mu.data(), 8 * H.mu.size(), cudaMemcpyHostToDevice, stream) != cudaSuccess ||
+         cudaMemcpyAsync(scratch + 8 * nl, H.list.data(), 4 * H.list.size(), cudaMemcpyHostToDevice,
+                         stream) != cudaSuccess))
+        rc = -1;
+    if (!rc) rc = enqueue(H, a, stream);
+    // (copies from pageable host memory are staged before cudaMemcpyAsync returns, so the
+    // host vectors may go out of scope here)
+    cudaFreeAsync(scratch, stream);
+    return rc;
+}
+
+// A sieve prepared once and launched many times (the device tables stay allocated):
+// enqueue_sieve_plan only launches kernels, so it can be captured in a CUDA graph.
+struct SievePlan {
+    SieveHost H;
+    SieveArgs a;
+    uint8_t* table = nullptr;
+};
+
+SievePlan* create_sieve_plan(const SieveArgs& a, int sms)
+{
+    SievePlan* P = new SievePlan;
+    P->a = a;
+    if (a.seg_hi > a.seg_lo && analyse(a, sms, P->H)) {
+        delete P;
+        return nullptr;
+    }
+    const size_t nl = P->H.list.empty() ? 1 : P->H.list.size();
+    if (cudaMalloc(&P->table, 12 * nl + 16) != cudaSuccess) {
+        cudaGetLastError();
+        delete P;
+        return nullptr;
+    }
+    P->H.T.mu = (const uint64_t*)P->table;
+    P->H.T.primes = (const uint32_t*)(P->table + 8 * nl);
+    if (!P->H.list.empty() &&
+        (cudaMemcpy(P->table, P->H.mu.data(), 8 * P->H.mu.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(P->table + 8 * nl, P->H.list.data(), 4 * P->H.list.size(), cudaMemcpyHostToDevice) !=
+             cudaSuccess)) {
+        cudaFree(P->table);
+        delete P;
+        return nullptr;
+    }
+    return P;
+}
+
+int enqueue_sieve_plan(const SievePlan* P, cudaStream_t stream)
+{
+    if (P->a.seg_hi <= P->a.seg_lo) return 0;
+    return enqueue(P->H, P->a, stream);
+}
+
+void destroy_sieve_plan(SievePlan* P)
+{
+    if (!P) return;
+    if (P->table) cudaFree(P->table);
+    delete P;
 }
 
 }  // namespace ffb

@@ -21,6 +21,14 @@ class GpuRecord(ctypes.Structure):
                 ("high", ctypes.c_uint64), ("tag", ctypes.c_uint8)]
 
 
+class FfbBatchInfo(ctypes.Structure):
+    _fields_ = [("ranges", ctypes.c_uint32), ("intervals", ctypes.c_uint32),
+                ("sums", ctypes.c_uint64), ("mapMaxValue", ctypes.c_uint64),
+                ("mapBytes", ctypes.c_uint64), ("sieveTileBytes", ctypes.c_uint32),
+                ("searchWarps", ctypes.c_uint32), ("autotuned", ctypes.c_int),
+                ("sieveMs", ctypes.c_float), ("searchMs", ctypes.c_float)]
+
+
 class FfbGeometry(ctypes.Structure):
     _fields_ = [("sumStart", ctypes.c_uint32), ("sumLimit", ctypes.c_uint32),
                 ("maxPrimeMapValue", ctypes.c_uint64), ("mapBytes", ctypes.c_uint64),
@@ -81,6 +89,14 @@ SIGNATURES = {
     "ffb_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
                                ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]),
     "ffb_free": (None, [ctypes.c_void_p]),
+    "ffb_batch_create": (ctypes.c_void_p, [ctypes.c_int, ctypes.c_uint32,
+                                           ctypes.POINTER(ctypes.c_int32),
+                                           ctypes.POINTER(ctypes.c_int32), ctypes.c_int]),
+    "ffb_batch_launch": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    "ffb_batch_collect": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                         ctypes.POINTER(ctypes.c_size_t)]),
+    "ffb_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FfbBatchInfo)]),
+    "ffb_batch_destroy": (None, [ctypes.c_void_p]),
 }
 
 _lib = None
@@ -151,3 +167,52 @@ def take_errors(dev=0):
     if lib.ffb_take_errors(dev, ctypes.byref(f)) != 0:
         raise RuntimeError("ffb_take_errors failed")
     return f.value
+
+
+class Batch:
+    """ffb_batch_*: many ranges (start, limit) evaluated together; .run() -> list of texts."""
+
+    def __init__(self, ranges, dev=0, autotune=True):
+        self.lib = load()
+        n = len(ranges)
+        self.n = n
+        s = (ctypes.c_int32 * n)(*[int(a) for a, _ in ranges])
+        l = (ctypes.c_int32 * n)(*[int(b) for _, b in ranges])
+        self.h = self.lib.ffb_batch_create(dev, n, s, l, 1 if autotune else 0)
+        if not self.h:
+            raise RuntimeError("ffb_batch_create failed")
+
+    def launch(self, stream=None):
+        if self.lib.ffb_batch_launch(self.h, stream) != 0:
+            raise RuntimeError("ffb_batch_launch failed")
+
+    def collect(self):
+        p = ctypes.c_void_p()
+        off = (ctypes.c_size_t * (self.n + 1))()
+        if self.lib.ffb_batch_collect(self.h, ctypes.byref(p), off) != 0:
+            raise RuntimeError("ffb_batch_collect failed")
+        try:
+            raw = ctypes.string_at(p, off[self.n])
+        finally:
+            self.lib.ffb_free(p)
+        return [raw[off[i]:off[i + 1]] for i in range(self.n)]
+
+    def run(self):
+        self.launch()
+        return self.collect()
+
+    def info(self):
+        i = FfbBatchInfo()
+        self.lib.ffb_batch_info(self.h, ctypes.byref(i))
+        return {n: getattr(i, n) for n, _ in i._fields_}
+
+    def close(self):
+        if self.h:
+            self.lib.ffb_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

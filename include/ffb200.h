@@ -242,6 +242,34 @@ typedef struct FfbContext FfbContext;
 FfbContext* ffb_context_create(int deviceIndex);
 void ffb_context_destroy(FfbContext* ctx);
 
+/* A batch of ff_sieve runs (no reference counterpart): n ranges, each given as the two
+ * atoi()-style arguments of `ff_sieve <sumStart> <sumLimit>`, evaluated together. One prime
+ * map is sieved for the whole batch, the sums of all ranges' schedules are merged into
+ * disjoint intervals that one persistent search launch takes as its work queue (each shared
+ * sum evaluated once), and both launches are captured once into a CUDA graph. autotune != 0
+ * times the sieve tile sizes (64..216 KB) and search block sizes (4, 8, 16 warps) on the
+ * batch first (kept per map size and sum count for later batches). Each range's text is
+ * exactly what ff_seg prints for it; the timing lines carry the batch's sieve and search
+ * times. Allocates its device buffers at creation. */
+typedef struct FfbBatch FfbBatch;
+typedef struct {
+    uint32_t ranges, intervals;
+    uint64_t sums;              /* distinct odd sums evaluated */
+    uint64_t mapMaxValue, mapBytes;
+    uint32_t sieveTileBytes, searchWarps;
+    int autotuned;              /* 0 fixed defaults, 1 timed at creation, 2 reused */
+    float sieveMs, searchMs;    /* device times of the last completed launch */
+} FfbBatchInfo;
+FfbBatch* ffb_batch_create(int deviceIndex, uint32_t n, const int32_t* starts,
+                           const int32_t* limits, int autotune);
+/* Replays the graph on `stream` (NULL: the batch's own stream). Asynchronous. */
+int ffb_batch_launch(FfbBatch* b, void* stream);
+/* Waits for the launch, copies the records back and emits every range's text into one
+ * malloc'd buffer (free with ffb_free): range i is text[offsets[i] .. offsets[i+1]). */
+int ffb_batch_collect(FfbBatch* b, char** text, size_t* offsets);
+int ffb_batch_info(const FfbBatch* b, FfbBatchInfo* info);
+void ffb_batch_destroy(FfbBatch* b);
+
 /* The whole `ff_sieve` / ff_seg stdout for the given arguments (see ffb_geometry), with the
  * timing lines in microseconds ("Prime time: <us> μs", "Freudenthal time: <us> μs").
  * *text receives a malloc'd buffer (free with ffb_free), *len its length. ctx may be NULL
