@@ -251,6 +251,9 @@ def ours(args, rank, world, dist):
     batched = None
     if rank == 0 and world == 1 and not args.no_batched and LIMIT == 2097152:
         batched = batched_section(args, dev)
+    served = None
+    if rank == 0 and world == 1 and args.served_requests > 0 and LIMIT == 2097152:
+        served = served_section(args, dev)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -264,7 +267,7 @@ def ours(args, rank, world, dist):
                        "parallelism": f"sum shards x{world}" if world > 1 else "1 GPU"},
             "kernel_ms": {"sieve_tiles": sieve_ms, "search_kernel": search_ms},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "batched": batched,
+            "batched": batched, "served": served,
             "gpu_launches": 2 * args.steps,
         }
         print(json.dumps(line), flush=True)
@@ -327,6 +330,121 @@ def batched_section(args, dev):
             "plain_one_launch_per_range": {"value": plain, "unit": UNIT,
                                            "sample": f"{len(sample)} of the 256 ranges (every 16th)"},
             "vs_plain": value / plain}
+
+
+# ---------------------------------------------------------------------------------------
+# served mode: a Poisson stream of requests (seed 1) against the serving loop
+# ---------------------------------------------------------------------------------------
+def pct(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(round(q * (len(xs) - 1)))))
+    return xs[k]
+
+
+def serve_stream(ffb, dev, reqs, budget, **cfg):
+    """Submits reqs [(arrival_s, start, limit)] at their arrival times (arrival 0 = now) to a
+    fresh server, drains the output on a second thread; returns per-request figures."""
+    srv = ffb.Server(dev=dev, budget_bytes=budget, **cfg)
+    try:
+        got = {"bytes": 0, "chunks": 0, "done": 0, "failed": 0}
+
+        def consume():
+            while got["done"] + got["failed"] < len(reqs):
+                c = srv.next(1000, keep_text=False)
+                if c is None:
+                    continue
+                got["chunks"] += 1
+                got["bytes"] += c[3]
+                if c[2] == 1:
+                    got["done"] += 1
+                elif c[2] < 0:
+                    got["failed"] += 1
+        th = threading.Thread(target=consume, daemon=True)
+        th.start()
+        t0 = time.perf_counter()
+        ids = []
+        for t, a, b in reqs:
+            d = t0 + t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ids.append(srv.submit(a, b))
+        srv.drain()
+        th.join(timeout=60)
+        info = srv.info()
+        ri = [srv.request_info(i) for i in ids]
+    finally:
+        srv.close()
+    lat = [(r["doneUs"] - r["submitUs"]) / 1e3 for r in ri]
+    first = [(r["firstChunkUs"] - r["submitUs"]) / 1e3 for r in ri]
+    span_s = (max(r["doneUs"] for r in ri) - min(r["submitUs"] for r in ri)) / 1e6
+    sums = sum(r["sums"] for r in ri)
+    return {"requests": len(reqs), "sums": sums, "span_s": span_s, "value": sums / span_s,
+            "requests_per_s": len(reqs) / span_s,
+            "latency_ms": {"p50": pct(lat, 0.50), "p99": pct(lat, 0.99), "p999": pct(lat, 0.999),
+                           "max": max(lat)},
+            "first_chunk_ms": {"p50": pct(first, 0.50), "p99": pct(first, 0.99)},
+            "failed": got["failed"], "text_bytes": got["bytes"], "chunks": got["chunks"],
+            "launches": info["launches"], "sums_searched": info["sumsSearched"],
+            "search_device_ms": info["searchMs"], "sieve_device_ms": info["sieveMs"],
+            "map_bytes": info["mapBytes"], "map_max_value": info["mapMaxValue"],
+            "max_queued": info["maxQueued"], "budget_bytes": info["budget"]["budget"],
+            "stage1_probes": info["stage1Probes"], "stage2_items": info["stage2Items"],
+            "mr_candidates": info["mrCandidates"], "mr_base2_passed": info["mrBase2Passed"],
+            "backing_bytes": info["budget"]["backing"], "scratch_bytes": info["budget"]["scratch"]}
+
+
+def served_section(args, dev):
+    import ffb200 as ffb
+    import workloads
+    lib = ffb.load()
+    n = args.served_requests
+    budget = 8 << 30
+    base = workloads.served_requests(seed=1, n=10000, rate=1.0)[:n]
+    # capacity: the whole prefix at once
+    sat = serve_stream(ffb, dev, [(0.0, a, b) for _, a, b in base], budget)
+    cap_rps = sat["requests_per_s"]
+    runs = []
+    for frac in args.served_loads:
+        rate = frac * cap_rps
+        # the same requests, arrival gaps of the seed-1 stream rescaled to this rate
+        reqs = [(t / rate, a, b) for t, a, b in base]
+        r = serve_stream(ffb, dev, reqs, budget)
+        r["rate_per_s"] = rate
+        r["load"] = frac
+        runs.append(r)
+    # the plain method once per request (ffb_run: its own map sieved, then the search)
+    ctx = lib.ffb_context_create(dev)
+    sample = base[::max(1, n // args.served_plain)]
+    p, m = ctypes.c_void_p(), ctypes.c_size_t()
+    plain_t, plain_sums, plain_lat = 0.0, 0, []
+    try:
+        assert lib.ffb_run(ctx, 2, 5, 65536, ctypes.byref(p), ctypes.byref(m)) == 0
+        lib.ffb_free(p)
+        for _, a, b in sample:
+            s = time.perf_counter()
+            assert lib.ffb_run(ctx, 2, a, b, ctypes.byref(p), ctypes.byref(m)) == 0
+            dt = time.perf_counter() - s
+            lib.ffb_free(p)
+            plain_t += dt
+            plain_lat.append(1e3 * dt)
+            g, _ = ffb.geometry(a, b)
+            plain_sums += sum((min(l, g.sumLimit) - (f | 1)) // 2 + 1
+                              for f, l in ffb.schedule(g.sumStart, g.sumLimit, g.maxPrimeMapValue)
+                              if (f | 1) <= l)
+    finally:
+        lib.ffb_context_destroy(ctx)
+    plain = plain_sums / plain_t
+    return {"workload": f"first {n} of the 10,000 seed-1 requests (limit U{{69..2^22}}, "
+                        f"length floor(2^U[6,20]), start max(5, limit-length+1)); Poisson "
+                        f"arrivals of the seed-1 stream rescaled to each rate",
+            "budget": "8 GiB (computeBudget: f 0.90, cap 8 GiB)",
+            "saturation": sat, "rates": runs,
+            "plain_one_launch_per_request": {
+                "value": plain, "unit": UNIT, "latency_ms_p50": pct(plain_lat, 0.5),
+                "sample": f"{len(sample)} of the {n} requests, one ffb_run each"},
+            "vs_plain": sat["value"] / plain}
 
 
 # ---------------------------------------------------------------------------------------
@@ -439,6 +557,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the public-call timing")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-mode section")
+    ap.add_argument("--served-requests", type=int, default=400,
+                    help="requests of the seed-1 served stream to replay (0: skip)")
+    ap.add_argument("--served-loads", type=lambda v: [float(x) for x in v.split(",")],
+                    default=[0.5, 0.8], help="offered loads, as fractions of the measured capacity")
+    ap.add_argument("--served-plain", type=int, default=8,
+                    help="requests timed through the plain method for the comparison")
     ap.add_argument("--limit", type=int, default=2097152,
                     help="sumLimit of the job (2^21 for the reported line; smaller for profiling)")
     args = ap.parse_args()

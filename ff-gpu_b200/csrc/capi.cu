@@ -473,7 +473,7 @@ extern "C" int ffb_search_stats(int deviceIndex, uint64_t* out, int reset)
     FFB_CUDA(cudaSetDevice(deviceIndex));
     FFB_CUDA(cudaDeviceSynchronize());
     FFB_CUDA(cudaMemcpy(out, stats_words(s), 16, cudaMemcpyDeviceToHost));
-    if (reset) FFB_CUDA(cudaMemset(stats_words(s), 0, 16));
+    if (reset) FFB_CUDA(cudaMemset(stats_words(s), 0, 32));
     return 0;
 }
 

@@ -20,6 +20,7 @@
 //     list, its partially-sorted skip (reference/segmentedSieve.C:451) and its early
 //     returns are replayed exactly from the factorisation, since every IsPrime it makes on
 //     the cofactor is a pure function of the factorisation.
+#include "ffb200.h"
 #include "ffb_device.cuh"
 #include "ffb_internal.h"
 
@@ -36,14 +37,38 @@ struct Fac {
     int n;
 };
 
+// Prime::IsPrime for the search (reference/segmentedSieve.C:283-296). The map-only
+// variant is launched only when the map reaches every value the search can ask about; its
+// Miller-Rabin is the plain form, which it never reaches.
+template <bool kMR>
+__device__ __forceinline__ bool isp(const SearchArgs& A, uint64_t n)
+{
+    if (n == 2) return true;
+    if (!(n & 1)) return false;
+    if (n > A.bound) {
+        if constexpr (kMR) return miller_rabin(n, A.err);
+        else return miller_rabin_plain(n, A.err);
+    }
+    return (__ldg(A.map + (n >> 4)) >> (7 - ((n >> 1) & 7))) & 1;
+}
+
+// ProductOfTermPairsHasSingleFactorPair (reference/segmentedSieve.C:419-422).
+template <bool kMR>
+__device__ __forceinline__ bool pair1(const SearchArgs& A, uint64_t i)
+{
+    if (!(i & 1)) return true;
+    return isp<kMR>(A, i - 2);
+}
+
 // Ascending prime factorisation of an odd x < 2^32 by the exact-division table, with the
 // cofactor's primality read from the bitmap after every factor found.
+template <bool kMR>
 __device__ int factor_odd(uint32_t x, uint32_t* q, uint32_t* e, int cap, const SearchArgs& A)
 {
     int cnt = 0;
     uint32_t n = x;
     if (n <= 1) return 0;
-    if (is_prime(A.map, A.bound, n, A.err)) { q[0] = n; e[0] = 1; return 1; }
+    if (isp<kMR>(A, n)) { q[0] = n; e[0] = 1; return 1; }
     for (uint32_t i = 0; i < A.ntdiv; ++i) {
         const TDiv t = A.tdiv[i];
         if ((uint64_t)t.p * t.p > n) break;
@@ -54,7 +79,7 @@ __device__ int factor_odd(uint32_t x, uint32_t* q, uint32_t* e, int cap, const S
             if (cnt < cap) { q[cnt] = t.p; e[cnt] = ex; }
             ++cnt;
             if (n == 1) return cnt;
-            if (is_prime(A.map, A.bound, n, A.err)) {
+            if (isp<kMR>(A, n)) {
                 if (cnt < cap) { q[cnt] = n; e[cnt] = 1; }
                 return cnt + 1;
             }
@@ -67,11 +92,12 @@ __device__ int factor_odd(uint32_t x, uint32_t* q, uint32_t* e, int cap, const S
     return cnt;
 }
 
+template <bool kMR>
 __device__ void factor_product(uint32_t a, uint32_t b, Fac& f, const SearchArgs& A)
 {
     uint32_t qa[10], ea[10], qb[10], eb[10];
-    int na = factor_odd(a, qa, ea, 10, A);
-    int nb = b == 1 ? 0 : factor_odd(b, qb, eb, 10, A);
+    int na = factor_odd<kMR>(a, qa, ea, 10, A);
+    int nb = b == 1 ? 0 : factor_odd<kMR>(b, qb, eb, 10, A);
     int i = 0, j = 0, n = 0;
     while (i < na || j < nb) {
         uint32_t q, e;
@@ -87,6 +113,7 @@ __device__ void factor_product(uint32_t a, uint32_t b, Fac& f, const SearchArgs&
 // AllButOneProductOfTermPairsOfSumOfFactorPairsHasSingleFactorPair
 // (reference/segmentedSieve.C:424-477) replayed from the factorisation f of oddProduct.
 // F[i] are the divisors the reference stores in factors[], C[i] = product / F[i].
+template <bool kMR>
 __device__ __noinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const Fac& f,
                                          const SearchArgs& A)
 {
@@ -97,7 +124,7 @@ __device__ __noinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const
     F[0] = 1ull << k;
     C[0] = odd_product;
     if (F[0] <= lim) {
-        nm += !single_pair(A.map, A.bound, F[0] + C[0], A.err);
+        nm += !pair1<kMR>(A, F[0] + C[0]);
         nf = 1;
     }
     int idx = 0;
@@ -122,7 +149,7 @@ __device__ __noinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const
         for (uint32_t j = 0; j < e; ++j) {
             if (tf <= lim) {
                 const uint64_t ctf = (odd_product * tfi) << k;     // P / tf, exact
-                if ((nm += !single_pair(A.map, A.bound, tf + ctf, A.err)) > 1) return false;
+                if ((nm += !pair1<kMR>(A, tf + ctf)) > 1) return false;
                 if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return false; }
                 F[nf + npend] = tf;
                 C[nf + npend] = ctf;
@@ -131,7 +158,7 @@ __device__ __noinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const
                     const uint64_t m = F[g] * tf;
                     if (m <= lim) {
                         const uint64_t cm = C[g] * tfi;              // C[g] / tf, exact
-                        if ((nm += !single_pair(A.map, A.bound, m + cm, A.err)) > 1) return false;
+                        if ((nm += !pair1<kMR>(A, m + cm)) > 1) return false;
                         if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return false; }
                         F[nf + npend] = m;
                         C[nf + npend] = cm;
@@ -160,6 +187,7 @@ __device__ __forceinline__ uint32_t enc(uint32_t k, uint32_t o, bool comp)
 }
 
 // Stage 2: the split's AllButOne... verdict (DoesPeterKnow's last step, or Power2Composite).
+template <bool kMR>
 __device__ bool stage2(uint32_t item, uint32_t s, const SearchArgs& A, uint32_t* ta, uint32_t* tb)
 {
     const uint32_t k = item & 31;
@@ -167,32 +195,41 @@ __device__ bool stage2(uint32_t item, uint32_t s, const SearchArgs& A, uint32_t*
     uint64_t odd_product;
     if (item & 32) {
         const uint32_t odd = s - (1u << k);
-        factor_product(odd, 1, f, A);
+        factor_product<kMR>(odd, 1, f, A);
         odd_product = odd;
         *ta = 1u << k;
         *tb = odd;
     } else {
         const uint32_t o = item >> 6;
         const uint32_t even = o << k, b = s - even;
-        factor_product(o, b, f, A);
+        factor_product<kMR>(o, b, f, A);
         odd_product = (uint64_t)o * b;
         *ta = even;
         *tb = b;
     }
-    return all_but_one(k, odd_product, f, A);
+    return all_but_one<kMR>(k, odd_product, f, A);
 }
 
-// Stage 1: the probe of 2^k + o*b - 2 (DoesPeterKnow's first test).
-__device__ __forceinline__ bool stage1(uint32_t item, uint32_t s, const SearchArgs& A)
+// Stage 1: the pair sum 2^k + o*b whose probe 2^k + o*b - 2 is DoesPeterKnow's first test.
+__device__ __forceinline__ uint64_t stage1_value(uint32_t item, uint32_t s)
 {
     const uint32_t k = item & 31, o = item >> 6;
     const uint32_t b = s - (o << k);
-    return single_pair(A.map, A.bound, (1ull << k) + (uint64_t)o * b, A.err);
+    return (1ull << k) + (uint64_t)o * b;
 }
 
+// Per-warp queues of pending split items (shared memory). With the Miller-Rabin variant
+// a third queue holds the items whose probe lies above the map and survived the small-prime
+// test, so that Miller-Rabin always runs on 32 candidates at once. Each queue holds at most
+// 127 items: before any stage pushes, every queue holds fewer than 32 (settle() below),
+// a stage pushes at most 32 items in all, and a drain never outputs more than it takes,
+// so the total stays below 128.
+template <bool kMR>
 struct WarpQ {
-    uint32_t a[kQueue];
-    uint32_t b[kQueue];
+    static constexpr int kCap = kMR ? 128 : kQueue;
+    uint32_t a[kCap];
+    uint32_t b[kCap];
+    uint32_t c[kMR ? kCap : 1];
 };
 
 // Appends the items of the lanes with `pred` to q[n..]; returns the new size (uniform).
@@ -206,13 +243,27 @@ __device__ __forceinline__ uint32_t push(uint32_t* q, uint32_t n, bool pred, uin
 
 struct SumState {
     uint32_t s;
-    uint32_t count;   // valid splits seen so far (saturating use: >= 2 means rejected)
-    uint32_t ta, tb;  // terms of the first valid split
-    uint32_t na, nb;  // queue sizes
+    uint32_t count;       // valid splits seen so far (saturating use: >= 2 means rejected)
+    uint32_t ta, tb;      // terms of the first valid split
+    uint32_t na, nb, nc;  // queue sizes
 };
 
-// Runs stage 1 on up to 32 queued items, moving the survivors to queue b.
-__device__ void drain_a(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
+// single_pair(i) as far as it is decided without Miller-Rabin: 0 false, 1 true, 2 the probe
+// i - 2 lies above the map and has no factor below 64 (Miller-Rabin decides).
+__device__ __forceinline__ int pair_class(const SearchArgs& A, uint64_t i)
+{
+    if (!(i & 1)) return 1;
+    const uint64_t n = i - 2;
+    if (n <= A.bound) return (__ldg(A.map + (n >> 4)) >> (7 - ((n >> 1) & 7))) & 1;
+    if (n >= (1ull << 48)) atomicOr(A.err, kErrMrDomain);
+    if (n > 61 && small_factor(n)) return 0;
+    return 2;
+}
+
+// Runs stage 1 on up to 32 queued items: passes go to queue b; with the Miller-Rabin variant,
+// probes above the map go to queue c.
+template <bool kMR>
+__device__ void drain_a(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int lane)
 {
     const uint32_t take = st.na < 32 ? st.na : 32;
     const uint32_t base = st.na - take;
@@ -221,12 +272,45 @@ __device__ void drain_a(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
     const uint32_t item = act ? Q.a[base + lane] : 0;
     __syncwarp();
     st.na = base;
-    const bool pass = act && stage1(item, st.s, A);
-    st.nb = push(Q.b, st.nb, pass, item, lane);
+    const uint64_t v = act ? stage1_value(item, st.s) : 0;
+    if (kMR) {
+        const int cls = act ? pair_class(A, v) : 0;
+        st.nb = push(Q.b, st.nb, cls == 1, item, lane);
+        st.nc = push(Q.c, st.nc, cls == 2, item, lane);
+    } else {
+        const bool pass = act && pair1<kMR>(A, v);
+        st.nb = push(Q.b, st.nb, pass, item, lane);
+    }
+}
+
+// Miller-Rabin on up to 32 queued probes at once (bit 5 of an item marks a stage-0 probe
+// o + b*2^k - 2, else it is the stage-1 probe 2^k + o*b - 2): stage-0 passes go on to queue
+// a, stage-1 passes to queue b.
+template <bool kMR>
+__device__ void drain_c(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int lane)
+{
+    const uint32_t take = st.nc < 32 ? st.nc : 32;
+    const uint32_t base = st.nc - take;
+    const bool act = (uint32_t)lane < take;
+    const uint32_t item = act ? Q.c[base + lane] : 0;
+    __syncwarp();
+    st.nc = base;
+    uint64_t n = 0;
+    if (act) {
+        const uint32_t k = item & 31, o = item >> 6;
+        const uint32_t b = st.s - (o << k);
+        n = (item & 32) ? o + ((uint64_t)b << k) - 2 : (1ull << k) + (uint64_t)o * b - 2;
+    }
+    unsigned long long* cnt = lane == 0 ? A.stats : nullptr;
+    const bool prime = mr_rounds(n, act, lane, cnt);
+    const bool from0 = (item & 32) != 0;
+    st.na = push(Q.a, st.na, prime && from0, item & ~32u, lane);
+    st.nb = push(Q.b, st.nb, prime && !from0, item, lane);
 }
 
 // Runs stage 2 on up to 32 queued items and adds the valid ones to the count.
-__device__ void drain_b(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
+template <bool kMR>
+__device__ void drain_b(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int lane)
 {
     const uint32_t take = st.nb < 32 ? st.nb : 32;
     const uint32_t base = st.nb - take;
@@ -236,7 +320,7 @@ __device__ void drain_b(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
     __syncwarp();
     st.nb = base;
     uint32_t a = 0, b = 0;
-    const bool valid = act && stage2(item, st.s, A, &a, &b);
+    const bool valid = act && stage2<kMR>(item, st.s, A, &a, &b);
     const uint32_t m = __ballot_sync(0xFFFFFFFFu, valid);
     if (m) {
         const int src = __ffs(m) - 1;
@@ -247,29 +331,47 @@ __device__ void drain_b(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
     }
 }
 
-// Stage 0 of a Power2Odd split (reference/segmentedSieve.C:573-586 and the cheap probe of
-// DoesPeterKnow :636): o*b not a multiple of 3, and o == b or o + b*2^k - 2 prime.
-__device__ __forceinline__ bool stage0_odd(uint32_t s, uint32_t k, uint32_t o, const SearchArgs& A)
+// Drains every queue that holds 32 or more items (b first: it may reject the sum and pushes
+// nothing). Returns false once the sum is rejected.
+template <bool kMR>
+__device__ __forceinline__ bool settle(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int lane)
 {
-    const uint32_t b = s - (o << k);
-    if (o % 3 == 0 || b % 3 == 0) return false;
-    return o == b || single_pair(A.map, A.bound, o + ((uint64_t)b << k), A.err);
+    for (;;) {
+        if (st.nb >= 32) {
+            drain_b(st, Q, A, lane);
+            if (st.count > 1) return false;
+        } else if (kMR && st.nc >= 32) {
+            drain_c(st, Q, A, lane);
+        } else if (st.na >= 32) {
+            drain_a(st, Q, A, lane);
+        } else {
+            return true;
+        }
+    }
 }
 
-// Stage 0 of a Power2Even split (reference/segmentedSieve.C:614-627): o*b a multiple of 3
-// or b prime; then the cheap probe.
-__device__ __forceinline__ bool stage0_even(uint32_t s, uint32_t k, uint32_t o, const SearchArgs& A)
+// Stage 0 of a split. Power2Odd (reference/segmentedSieve.C:573-586): o*b not a multiple of
+// 3. Power2Even (:614-627): o*b a multiple of 3 or b prime. Then, in both, the cheap probe
+// of DoesPeterKnow (:636): o == b or o + b*2^k - 2 prime. Returns 0 rejected, 1 passed,
+// 2 the probe waits for Miller-Rabin (only when kMR).
+template <bool kOdd, bool kMR>
+__device__ __forceinline__ int stage0(uint32_t s, uint32_t k, uint32_t o, const SearchArgs& A)
 {
     const uint32_t b = s - (o << k);
-    if (o % 3 != 0 && b % 3 != 0 && !is_prime(A.map, A.bound, b, A.err)) return false;
-    return o == b || single_pair(A.map, A.bound, o + ((uint64_t)b << k), A.err);
+    const bool pre = kOdd ? (o % 3 != 0 && b % 3 != 0)
+                          : (o % 3 == 0 || b % 3 == 0 || isp<kMR>(A, b));
+    if (!pre) return 0;
+    if (o == b) return 1;
+    const uint64_t v = o + ((uint64_t)b << k);
+    if (kMR) return pair_class(A, v);
+    return pair1<kMR>(A, v) ? 1 : 0;
 }
 
 // Enumerates the splits of one phase for sum s: k = kfirst, kfirst+2, ... while o0<<k < s-2;
 // for each k the odd parts o = o0, o0+2, ... with o<<k < s-2. Returns false once the sum
 // is rejected (two valid splits).
-template <bool kOdd>
-__device__ bool run_phase(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
+template <bool kOdd, bool kMR>
+__device__ bool run_phase(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int lane)
 {
     const uint32_t s = st.s;
     const uint32_t o0 = kOdd ? 5 : 3;
@@ -280,10 +382,12 @@ __device__ bool run_phase(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
         for (uint32_t base = 0; base < n; base += 32) {
             const uint32_t i = base + lane;
             const uint32_t o = o0 + 2 * i;
-            const bool act = i < n;
-            const bool pass = act && (kOdd ? stage0_odd(s, k, o, A) : stage0_even(s, k, o, A));
-            st.na = push(Q.a, st.na, pass, enc(k, o, false), lane);
-            if (st.na >= 32) {
+            const int cls = i < n ? stage0<kOdd, kMR>(s, k, o, A) : 0;
+            st.na = push(Q.a, st.na, cls == 1, enc(k, o, false), lane);
+            if constexpr (kMR) {
+                st.nc = push(Q.c, st.nc, cls == 2, enc(k, o, true), lane);
+                if (!settle(st, Q, A, lane)) return false;
+            } else if (st.na >= 32) {
                 drain_a(st, Q, A, lane);
                 if (st.nb >= 32) {
                     drain_b(st, Q, A, lane);
@@ -295,12 +399,13 @@ __device__ bool run_phase(SumState& st, WarpQ& Q, const SearchArgs& A, int lane)
     return true;
 }
 
+template <bool kMR>
 __device__ void write_result(const SearchArgs& A, uint32_t s, uint32_t ri, uint32_t ta, uint32_t tb)
 {
     uint32_t lo = ta < tb ? ta : tb, hi = ta < tb ? tb : ta;
     if (A.rec) {
-        const bool lp = is_prime(A.map, A.bound, lo, A.err);
-        const bool hp = is_prime(A.map, A.bound, hi, A.err);
+        const bool lp = isp<kMR>(A, lo);
+        const bool hp = isp<kMR>(A, hi);
         A.rec[ri] = ((uint64_t)(lo | (lp ? 0x80000000u : 0u)) << 32) |
                                  (uint64_t)(hi | (hp ? 0x80000000u : 0u));
     }
@@ -315,12 +420,12 @@ __device__ void write_result(const SearchArgs& A, uint32_t s, uint32_t ri, uint3
     }
 }
 
-template <int W>
+template <int W, bool kMR>
 __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
 {
-    __shared__ WarpQ queues[W];
+    __shared__ WarpQ<kMR> queues[W];
     const int lane = threadIdx.x & 31;
-    WarpQ& Q = queues[threadIdx.x >> 5];
+    WarpQ<kMR>& Q = queues[threadIdx.x >> 5];
     const uint32_t nchunks = A.nseg ? A.nchunks : (A.nsums + 31) / 32;
     for (;;) {
         uint32_t c = 0;
@@ -359,13 +464,13 @@ __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
         if (act) {
             // Sammy's first statement (reference/segmentedSieve.C:805-806)
             const uint32_t d3 = s / 3;
-            bool pass = !single_pair(A.map, A.bound, s, A.err) &&
-                        (s != 3 * d3 || is_prime(A.map, A.bound, d3, A.err));
+            bool pass = !pair1<kMR>(A, s) &&
+                        (s != 3 * d3 || isp<kMR>(A, d3));
             if (pass) {
                 // Power2Prime (reference/segmentedSieve.C:547-564)
                 for (uint32_t even = 4, k = 2; even < s - 2; even <<= 1, ++k) {
                     const uint32_t odd = s - even;
-                    if (is_prime(A.map, A.bound, odd, A.err)) {
+                    if (isp<kMR>(A, odd)) {
                         if (++cnt > 1) break;
                         if (cnt == 1) { ta = even; tb = odd; }
                     } else {
@@ -390,21 +495,33 @@ __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
             const uint32_t cmask = __shfl_sync(0xFFFFFFFFu, comp, src);
             st.na = 0;
             st.nb = 0;
+            st.nc = 0;
             // Power2Composite items (reference/segmentedSieve.C:591-605) go straight to stage 2
             st.nb = push(Q.b, 0, (cmask >> lane) & 1, enc(lane, 0, true), lane);
             bool open = true;
             if (st.nb >= 32) { drain_b(st, Q, A, lane); open = st.count <= 1; }
-            if (open) open = run_phase<true>(st, Q, A, lane);
-            if (open) open = run_phase<false>(st, Q, A, lane);
-            while (open && st.na > 0) {
-                drain_a(st, Q, A, lane);
-                if (st.nb >= 32) { drain_b(st, Q, A, lane); open = st.count <= 1; }
+            if (open) open = run_phase<true, kMR>(st, Q, A, lane);
+            if (open) open = run_phase<false, kMR>(st, Q, A, lane);
+            // flush the partly filled queues: stage 1, then Miller-Rabin, then stage 2
+            if constexpr (kMR) {
+                while (open) {
+                    if (st.na > 0) drain_a(st, Q, A, lane);
+                    else if (st.nc > 0) drain_c(st, Q, A, lane);
+                    else if (st.nb > 0) drain_b(st, Q, A, lane);
+                    else break;
+                    open = st.count <= 1 && settle(st, Q, A, lane);
+                }
+            } else {
+                while (open && st.na > 0) {
+                    drain_a(st, Q, A, lane);
+                    if (st.nb >= 32) { drain_b(st, Q, A, lane); open = st.count <= 1; }
+                }
+                while (open && st.nb > 0) {
+                    drain_b(st, Q, A, lane);
+                    open = st.count <= 1;
+                }
             }
-            while (open && st.nb > 0) {
-                drain_b(st, Q, A, lane);
-                open = st.count <= 1;
-            }
-            if (open && st.count == 1 && lane == 0) write_result(A, st.s, sri, st.ta, st.tb);
+            if (open && st.count == 1 && lane == 0) write_result<kMR>(A, st.s, sri, st.ta, st.tb);
             __syncwarp();
         }
     }
@@ -412,29 +529,33 @@ __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
 
 }  // namespace
 
-template <int W>
+template <int W, bool kMR>
 int launch_w(const SearchArgs& a, int sms, cudaStream_t stream)
 {
     int per_sm = 0;
-    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel<W>, W * 32, 0));
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel<W, kMR>, W * 32, 0));
     if (per_sm < 1) per_sm = 1;
     const uint32_t chunks = a.nseg ? a.nchunks : (a.nsums + 31) / 32;
     uint32_t blocks = (uint32_t)sms * (uint32_t)per_sm;
     const uint32_t need = (chunks + W - 1) / W;
     if (blocks > need) blocks = need;
     if (blocks == 0) return 0;
-    search_kernel<W><<<blocks, W * 32, 0, stream>>>(a);
+    search_kernel<W, kMR><<<blocks, W * 32, 0, stream>>>(a);
     FFB_CUDA(cudaGetLastError());
     return 0;
 }
 
+// The map-only kernel when the map reaches every value the sums up to a.hi probe (nothing
+// goes to Miller-Rabin in stages 0 and 1), else the variant that batches Miller-Rabin.
 int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
 {
     if (a.nseg == 0 && a.nsums == 0) return 0;
+    const uint64_t pb = ffb_probe_bound(a.hi);
+    const bool mr = pb == 0 || a.bound < pb;
     switch (a.warps) {
-    case 4: return launch_w<4>(a, sms, stream);
-    case 16: return launch_w<16>(a, sms, stream);
-    default: return launch_w<8>(a, sms, stream);
+    case 4: return mr ? launch_w<4, true>(a, sms, stream) : launch_w<4, false>(a, sms, stream);
+    case 16: return mr ? launch_w<16, true>(a, sms, stream) : launch_w<16, false>(a, sms, stream);
+    default: return mr ? launch_w<8, true>(a, sms, stream) : launch_w<8, false>(a, sms, stream);
     }
 }
 

@@ -35,6 +35,49 @@ class FfbGeometry(ctypes.Structure):
                 ("numPrimesRequested", ctypes.c_uint64), ("pmapSumLimit", ctypes.c_uint64)]
 
 
+class FfbBudget(ctypes.Structure):
+    """source/budget.h:23-33 (DeviceBudget)."""
+    _fields_ = [("fraction", ctypes.c_double), ("freeQueried", ctypes.c_ulonglong),
+                ("freeUsed", ctypes.c_ulonglong), ("cap", ctypes.c_ulonglong),
+                ("budget", ctypes.c_ulonglong), ("scratch", ctypes.c_ulonglong),
+                ("headroom", ctypes.c_ulonglong), ("backing", ctypes.c_ulonglong),
+                ("slabCount", ctypes.c_ulonglong)]
+
+
+class FfbServeConfig(ctypes.Structure):
+    _fields_ = [("vramBudgetBytes", ctypes.c_uint64), ("vramFraction", ctypes.c_double),
+                ("slots", ctypes.c_uint32), ("launchWork", ctypes.c_uint32),
+                ("launchSums", ctypes.c_uint32), ("searchWarps", ctypes.c_uint32),
+                ("warmLimit", ctypes.c_uint32)]
+
+
+class FfbServeChunk(ctypes.Structure):
+    _fields_ = [("request", ctypes.c_uint64), ("seq", ctypes.c_uint32), ("status", ctypes.c_int32),
+                ("text", ctypes.c_void_p), ("len", ctypes.c_size_t)]
+
+
+class FfbServeRequestInfo(ctypes.Structure):
+    _fields_ = [("sumStart", ctypes.c_uint32), ("sumLimit", ctypes.c_uint32),
+                ("sums", ctypes.c_uint64), ("textBytes", ctypes.c_uint64),
+                ("bodyHash", ctypes.c_uint64), ("submitUs", ctypes.c_double),
+                ("admitUs", ctypes.c_double), ("firstChunkUs", ctypes.c_double),
+                ("doneUs", ctypes.c_double), ("launches", ctypes.c_uint32),
+                ("state", ctypes.c_int32)]
+
+
+class FfbServeInfo(ctypes.Structure):
+    _fields_ = [("budget", FfbBudget), ("mapBytes", ctypes.c_uint64),
+                ("mapMaxValue", ctypes.c_uint64), ("requests", ctypes.c_uint64),
+                ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64), ("sumsRequested", ctypes.c_uint64),
+                ("sumsSearched", ctypes.c_uint64), ("chunks", ctypes.c_uint64),
+                ("textBytes", ctypes.c_uint64), ("slots", ctypes.c_uint32),
+                ("maxQueued", ctypes.c_uint32), ("sieveMs", ctypes.c_double),
+                ("searchMs", ctypes.c_double), ("stage1Probes", ctypes.c_uint64),
+                ("stage2Items", ctypes.c_uint64), ("mrCandidates", ctypes.c_uint64),
+                ("mrBase2Passed", ctypes.c_uint64)]
+
+
 # name -> (restype, argtypes); every symbol include/ffb200.h declares
 SIGNATURES = {
     "SieveSlabRun_sm_100a": (ctypes.c_int, [ctypes.c_int, u32p, ctypes.c_uint32, ctypes.c_uint64,
@@ -97,6 +140,21 @@ SIGNATURES = {
                                          ctypes.POINTER(ctypes.c_size_t)]),
     "ffb_batch_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FfbBatchInfo)]),
     "ffb_batch_destroy": (None, [ctypes.c_void_p]),
+    "ffb_compute_budget": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_double, ctypes.c_uint64,
+                                          ctypes.c_uint64, ctypes.c_uint64,
+                                          ctypes.POINTER(FfbBudget)]),
+    "ffb_shrink_budget": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_double, ctypes.c_uint64,
+                                         ctypes.c_uint64, ctypes.c_uint64,
+                                         ctypes.POINTER(FfbBudget)]),
+    "ffb_serve_create": (ctypes.c_void_p, [ctypes.c_int, ctypes.POINTER(FfbServeConfig)]),
+    "ffb_serve_submit": (ctypes.c_int64, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int32,
+                                          ctypes.c_int32]),
+    "ffb_serve_next": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FfbServeChunk), ctypes.c_int]),
+    "ffb_serve_request_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64,
+                                              ctypes.POINTER(FfbServeRequestInfo)]),
+    "ffb_serve_info": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(FfbServeInfo)]),
+    "ffb_serve_drain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    "ffb_serve_destroy": (None, [ctypes.c_void_p]),
 }
 
 _lib = None
@@ -209,6 +267,104 @@ class Batch:
     def close(self):
         if self.h:
             self.lib.ffb_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def _struct_dict(st):
+    out = {}
+    for n, _ in st._fields_:
+        v = getattr(st, n)
+        out[n] = _struct_dict(v) if isinstance(v, ctypes.Structure) else v
+    return out
+
+
+def compute_budget(free_bytes, fraction=0.90, cap=0, scratch=0, slab=1 << 30, shrink=False):
+    """computeBudget / shrinkFractionForAlloc of the reference as a dict."""
+    lib = load()
+    b = FfbBudget()
+    fn = lib.ffb_shrink_budget if shrink else lib.ffb_compute_budget
+    if fn(free_bytes, fraction, cap, scratch, slab, ctypes.byref(b)) != 0:
+        raise ValueError("bad budget arguments")
+    return _struct_dict(b)
+
+
+class Server:
+    """ffb_serve_*: submit(start, limit) -> id; next() -> (id, seq, status, bytes) chunks."""
+
+    def __init__(self, dev=0, budget_bytes=8 << 30, fraction=0.90, slots=0, launch_work=0,
+                 launch_sums=0, warps=0, warm_limit=0):
+        self.lib = load()
+        cfg = FfbServeConfig(budget_bytes, fraction, slots, launch_work, launch_sums, warps,
+                             warm_limit)
+        self.h = self.lib.ffb_serve_create(dev, ctypes.byref(cfg))
+        if not self.h:
+            raise RuntimeError("ffb_serve_create failed")
+
+    def submit(self, *args):
+        a = [int(x) for x in args] + [0, 0]
+        rid = self.lib.ffb_serve_submit(self.h, len(args), a[0], a[1])
+        if rid < 0:
+            raise ValueError(f"request {args} rejected")
+        return rid
+
+    def next(self, timeout_ms=-1, keep_text=True):
+        """(request, seq, status, text or length) or None on timeout."""
+        c = FfbServeChunk()
+        if self.lib.ffb_serve_next(self.h, ctypes.byref(c), timeout_ms) != 1:
+            return None
+        try:
+            body = ctypes.string_at(c.text, c.len) if (keep_text and c.text) else c.len
+        finally:
+            if c.text:
+                self.lib.ffb_free(c.text)
+        return c.request, c.seq, c.status, body
+
+    def collect(self, ids, timeout_ms=600000):
+        """Texts of the given requests (bytes, None when failed), in the order of ids."""
+        want = set(ids)
+        parts = {i: [] for i in ids}
+        failed = set()
+        done = set()
+        while done | failed != want:
+            got = self.next(timeout_ms)
+            if got is None:
+                raise TimeoutError("no output within the timeout")
+            rid, seq, status, text = got
+            if rid not in parts:
+                continue
+            if status < 0:
+                failed.add(rid)
+                continue
+            if seq != len(parts[rid]):
+                raise RuntimeError(f"request {rid}: chunk {seq} out of order")
+            parts[rid].append(text)
+            if status == 1:
+                done.add(rid)
+        return [None if i in failed else b"".join(parts[i]) for i in ids]
+
+    def request_info(self, rid):
+        o = FfbServeRequestInfo()
+        if self.lib.ffb_serve_request_info(self.h, rid, ctypes.byref(o)) != 0:
+            raise KeyError(rid)
+        return _struct_dict(o)
+
+    def info(self):
+        o = FfbServeInfo()
+        self.lib.ffb_serve_info(self.h, ctypes.byref(o))
+        return _struct_dict(o)
+
+    def drain(self, timeout_ms=-1):
+        return self.lib.ffb_serve_drain(self.h, timeout_ms) == 0
+
+    def close(self):
+        if self.h:
+            self.lib.ffb_serve_destroy(self.h)
             self.h = None
 
     def __enter__(self):

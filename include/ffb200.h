@@ -270,6 +270,104 @@ int ffb_batch_collect(FfbBatch* b, char** text, size_t* offsets);
 int ffb_batch_info(const FfbBatch* b, FfbBatchInfo* info);
 void ffb_batch_destroy(FfbBatch* b);
 
+/* ---------------------------------------------------------------------------------- */
+/* Device memory budget (source/budget.h:23-46, source/budget.cpp:15-51): the         */
+/* reference's DeviceBudget and its computeBudget / shrinkFractionForAlloc, as plain   */
+/* functions of the free bytes (the reference reads them from a DeviceInfo).           */
+/* ---------------------------------------------------------------------------------- */
+typedef struct {
+    double fraction;                /* f actually used */
+    unsigned long long freeQueried; /* free device bytes given */
+    unsigned long long freeUsed;    /* floor(f x free) */
+    unsigned long long cap;         /* ~0 when uncapped */
+    unsigned long long budget;      /* min(freeUsed, cap) */
+    unsigned long long scratch;     /* fixed, else min(floor(0.15 x budget), 1 GiB) */
+    unsigned long long headroom;    /* 64 MiB */
+    unsigned long long backing;     /* budget - scratch - headroom, floored to 4 KiB */
+    unsigned long long slabCount;   /* floor(backing / slab bytes) */
+} FfbBudget;
+/* computeBudget (source/budget.cpp:15-42). capBytes 0 = no cap (the reference's
+ * hasBudgetCap false), scratchBytes 0 = the automatic scratch, slabBytes 0 = no slab count.
+ * Returns -1 when fraction is outside (0, 1]. */
+int ffb_compute_budget(uint64_t freeBytes, double fraction, uint64_t capBytes,
+                       uint64_t scratchBytes, uint64_t slabBytes, FfbBudget* out);
+/* shrinkFractionForAlloc (source/budget.cpp:44-51): the budget at the midpoint between
+ * fraction and the 0.50 floor (at or below the floor: the floor itself). */
+int ffb_shrink_budget(uint64_t freeBytes, double fraction, uint64_t capBytes,
+                      uint64_t scratchBytes, uint64_t slabBytes, FfbBudget* out);
+
+/* ---------------------------------------------------------------------------------- */
+/* Serving loop (no reference counterpart): ff_sieve requests of any size submitted    */
+/* while others run. The device keeps one prime map resident (sieved at creation up to */
+/* the bound the first requests need, grown to the largest admitted limit, never past  */
+/* the budget's backing bytes; Miller-Rabin answers probes above it, so every answer is */
+/* the same as with the reference's own map), the trial-division table and, per launch */
+/* slot, record and work-queue buffers carved from the budget's scratch bytes.          */
+/* Continuous batching: whenever a launch slot is free, the scheduler fills one search  */
+/* launch with a slice of every waiting request (oldest first, each request's sums in   */
+/* its emission order, equal shares of the launch's work), so requests that arrive      */
+/* while others are on the GPU join the next launch and their work overlaps on the      */
+/* device. Each request's text is exactly ff_seg's stdout for its arguments, streamed   */
+/* back in that order as chunks; its timing lines carry the sieve time its admission    */
+/* caused and its time from admission to completion.                                    */
+/* ---------------------------------------------------------------------------------- */
+typedef struct FfbServer FfbServer;
+typedef struct {
+    uint64_t vramBudgetBytes;   /* budget cap (the reference's --vram-budget); 0 = none */
+    double vramFraction;        /* f of the free device memory; 0 = 0.90 */
+    uint32_t slots;             /* launches in flight; 0 = 3 */
+    uint32_t launchWork;        /* work of one launch in odd sums at sum 2^21 (a sum s counts
+                                   s/2^21); 0 = 65536 */
+    uint32_t launchSums;        /* most odd sums of one launch; 0 = 2^22 */
+    uint32_t searchWarps;       /* warps per search block: 4, 8 or 16; 0 = 16 */
+    uint32_t warmLimit;         /* sieve the map for sums up to this at creation; 0 = none */
+} FfbServeConfig;
+typedef struct {
+    uint64_t request;           /* id returned by ffb_serve_submit */
+    uint32_t seq;               /* 0, 1, ... within the request */
+    int32_t status;             /* 1 the request's last chunk, 0 more follow, -1 failed */
+    char* text;                 /* malloc'd (ffb_free); the request's next bytes */
+    size_t len;
+} FfbServeChunk;
+typedef struct {
+    uint32_t sumStart, sumLimit;    /* after the reference's argument handling */
+    uint64_t sums;                  /* odd sums in its schedule */
+    uint64_t textBytes;             /* bytes delivered so far */
+    uint64_t bodyHash;              /* FNV-1a 64 of its solution lines */
+    double submitUs, admitUs, firstChunkUs, doneUs;  /* since the server's creation */
+    uint32_t launches;              /* launches its sums were spread over */
+    int32_t state;                  /* 0 queued, 1 running, 2 done, -1 failed */
+} FfbServeRequestInfo;
+typedef struct {
+    FfbBudget budget;
+    uint64_t mapBytes, mapMaxValue;       /* the resident map's sieved part */
+    uint64_t requests, completed, failed;
+    uint64_t launches, sumsRequested, sumsSearched;
+    uint64_t chunks, textBytes;
+    uint32_t slots, maxQueued;            /* most requests waiting at once */
+    double sieveMs, searchMs;             /* device time of all sieve / search launches */
+    uint64_t stage1Probes;                /* probes of 2^k + o*b - 2 */
+    uint64_t stage2Items;                 /* AllButOne... evaluations */
+    uint64_t mrCandidates;                /* probes above the map given to the batched
+                                             Miller-Rabin (after the small-prime test) */
+    uint64_t mrBase2Passed;               /* of those, strong probable primes to base 2 */
+} FfbServeInfo;
+/* NULL (and a stderr line) when the budget leaves no room for the map and the slots. */
+FfbServer* ffb_serve_create(int deviceIndex, const FfbServeConfig* cfg);
+/* Queues `ff_sieve <a1> <a2>` (nargs positional arguments); returns its id (>= 0), or -1
+ * when the reference would not run the range or its sums exceed 2^25. */
+int64_t ffb_serve_submit(FfbServer* s, int nargs, int32_t a1, int32_t a2);
+/* The next chunk of output of any request (chunks of one request arrive in order).
+ * Returns 1 with *out filled, 0 when none came within timeoutMs (< 0: wait forever). */
+int ffb_serve_next(FfbServer* s, FfbServeChunk* out, int timeoutMs);
+int ffb_serve_request_info(FfbServer* s, uint64_t id, FfbServeRequestInfo* out);
+int ffb_serve_info(FfbServer* s, FfbServeInfo* out);
+/* Waits until every submitted request has completed or failed (timeoutMs < 0: forever).
+ * Returns 0, or 1 on timeout. */
+int ffb_serve_drain(FfbServer* s, int timeoutMs);
+/* Finishes the launches in flight, drops undelivered output and frees everything. */
+void ffb_serve_destroy(FfbServer* s);
+
 /* The whole `ff_sieve` / ff_seg stdout for the given arguments (see ffb_geometry), with the
  * timing lines in microseconds ("Prime time: <us> μs", "Freudenthal time: <us> μs").
  * *text receives a malloc'd buffer (free with ffb_free), *len its length. ctx may be NULL
