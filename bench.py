@@ -101,21 +101,6 @@ class ClockSampler:
 # ---------------------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------------------
-def shard_bounds(lo, hi, world, rank):
-    """Contiguous shard [a, b] of the odd sums lo..hi for `rank`, balanced by the search
-    cost, which grows about linearly with the sum (the cumulative cost ~ s^2)."""
-    import math
-    if world == 1:
-        return lo, hi
-
-    def cut(q):  # sum s with (s^2 - lo^2) / (hi^2 - lo^2) = q, made odd
-        s = int(math.sqrt(lo * lo + q * (hi * hi - lo * lo)))
-        return max(lo, min(hi, s | 1))
-    a = lo if rank == 0 else cut(rank / world)
-    b = hi if rank == world - 1 else cut((rank + 1) / world) - 2
-    return a, b
-
-
 def geometry_for(ffb, limit):
     g, _ = ffb.geometry(5, limit)
     return g
@@ -124,6 +109,7 @@ def geometry_for(ffb, limit):
 def ours(args, rank, world, dist):
     import torch
     import ffb200 as ffb
+    from shard import shard_bounds, gather_records
     lib = ffb.load()
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
@@ -184,11 +170,7 @@ def ours(args, rank, world, dist):
     stage2_per_step = stats[1] // args.steps
     # records of all shards to rank 0 (the exchange of the sharded job)
     if dist and world > 1:
-        sizes = [odd_sums(*shard_bounds(lo, hi, world, r)) for r in range(world)]
-        buf = torch.zeros(max(sizes), dtype=torch.int64, device="cuda")
-        buf[:nsums] = d_rec[:nsums]
-        gathered = [torch.empty_like(buf) for _ in range(world)]
-        dist.all_gather(gathered, buf)
+        gather_records(dist, d_rec, lo, hi, world, rank)
     t = torch.tensor([total_ms, sieve_ms, search_ms], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

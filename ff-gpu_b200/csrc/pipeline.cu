@@ -230,3 +230,46 @@ extern "C" int ffb_run(FfbContext* ctx, int nargs, int32_t a1, int32_t a2, char*
     *len = n;
     return 0;
 }
+
+extern "C" int ffb_emit(int nargs, int32_t a1, int32_t a2, const uint64_t* h_rec, uint32_t recLo,
+                        uint64_t nrec, double primeUs, double freudUs, char** text, size_t* len)
+{
+    if (!text || !len) return -1;
+    *text = nullptr;
+    *len = 0;
+    uint32_t start, limit;
+    parse_args(nargs, a1, a2, &start, &limit);
+    char hdr[2048];
+    Geometry g;
+    const int hn = plan_geometry(start, limit, &g, hdr, sizeof hdr);
+    std::vector<Range> ranges;
+    if (hn < 0 || !plan_schedule(start, limit, g.mpv, kThreads, ranges)) {
+        std::fprintf(stderr, "ffb_emit: arguments (%d, %d) cannot be run\n", a1, a2);
+        return -1;
+    }
+    const uint64_t rec_hi = (uint64_t)recLo + 2 * (nrec ? nrec - 1 : 0);
+    for (const Range& r : ranges) {
+        const uint32_t f = r.first | 1u;
+        if (f > r.last) continue;
+        const uint32_t l = r.last - !(r.last & 1);
+        if (!(recLo & 1) || nrec == 0 || !h_rec || f < recLo || l > rec_hi) {
+            std::fprintf(stderr, "ffb_emit: the records (odd sums %u..%llu) do not cover sums "
+                         "%u..%u of the schedule\n", recLo, (unsigned long long)rec_hi, f, l);
+            return -1;
+        }
+    }
+    const std::string body = emit(ranges, h_rec, recLo);
+    char tail[160];
+    const int tn = std::snprintf(tail, sizeof tail, "Prime time: %llu \xce\xbcs\nFreudenthal time: %llu \xce\xbcs\n",
+                                 (unsigned long long)primeUs, (unsigned long long)freudUs);
+    const size_t n = (size_t)hn + body.size() + (size_t)tn;
+    char* out = (char*)std::malloc(n + 1);
+    if (!out) return -1;
+    std::memcpy(out, hdr, (size_t)hn);
+    std::memcpy(out + hn, body.data(), body.size());
+    std::memcpy(out + hn + body.size(), tail, (size_t)tn);
+    out[n] = 0;
+    *text = out;
+    *len = n;
+    return 0;
+}

@@ -132,6 +132,9 @@ SIGNATURES = {
     "ffb_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
                                ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]),
     "ffb_free": (None, [ctypes.c_void_p]),
+    "ffb_emit": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
+                                ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
+                                ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]),
     "ffb_batch_create": (ctypes.c_void_p, [ctypes.c_int, ctypes.c_uint32,
                                            ctypes.POINTER(ctypes.c_int32),
                                            ctypes.POINTER(ctypes.c_int32), ctypes.c_int]),
@@ -213,6 +216,25 @@ def run(*args, ctx=None):
     rc = lib.ffb_run(ctx, len(args), *(list(args) + [0, 0])[:2], ctypes.byref(p), ctypes.byref(n))
     if rc != 0:
         raise RuntimeError(f"ffb_run{args} failed")
+    try:
+        return ctypes.string_at(p, n.value)
+    finally:
+        lib.ffb_free(p)
+
+
+def emit(args, records, rec_lo, prime_us=0.0, freud_us=0.0):
+    """ffb_emit: ff_seg's stdout from packed records (numpy uint64/int64 array, odd sums from
+    rec_lo) computed elsewhere."""
+    import numpy as np
+    lib = load()
+    rec = np.ascontiguousarray(records).view(np.uint64)
+    p = ctypes.c_void_p()
+    n = ctypes.c_size_t()
+    a = [int(x) for x in args] + [0, 0]
+    rc = lib.ffb_emit(len(args), a[0], a[1], rec.ctypes.data, rec_lo, rec.size, prime_us,
+                      freud_us, ctypes.byref(p), ctypes.byref(n))
+    if rc != 0:
+        raise ValueError(f"ffb_emit{tuple(args)} failed")
     try:
         return ctypes.string_at(p, n.value)
     finally:

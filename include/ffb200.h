@@ -373,6 +373,14 @@ void ffb_serve_destroy(FfbServer* s);
  * *text receives a malloc'd buffer (free with ffb_free), *len its length. ctx may be NULL
  * (a temporary context is used). */
 int ffb_run(FfbContext* ctx, int nargs, int32_t a1, int32_t a2, char** text, size_t* len);
+
+/* The ff_sieve / ff_seg stdout for the given arguments from packed records already computed
+ * (host memory, the format of ffb_search_async: h_rec[(s-recLo)/2] for odd sums
+ * s = recLo, recLo+2, ..., covering every sum of the schedule), with the given timing
+ * values in the last two lines. No device work: the host side of a job whose sums were
+ * searched elsewhere, e.g. in shards on several GPUs and gathered. */
+int ffb_emit(int nargs, int32_t a1, int32_t a2, const uint64_t* h_rec, uint32_t recLo,
+             uint64_t nrec, double primeUs, double freudUs, char** text, size_t* len);
 void ffb_free(void* p);
 
 #ifdef __cplusplus
