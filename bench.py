@@ -236,6 +236,9 @@ def ours(args, rank, world, dist):
     served = None
     if rank == 0 and world == 1 and args.served_requests > 0 and LIMIT == 2097152:
         served = served_section(args, dev)
+    sweep = None
+    if rank == 0 and world == 1 and not args.no_sieve_sweep and LIMIT == 2097152:
+        sweep = sieve_sweep_section(args, dev, hbm_peak)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -249,7 +252,7 @@ def ours(args, rank, world, dist):
                        "parallelism": f"sum shards x{world}" if world > 1 else "1 GPU"},
             "kernel_ms": {"sieve_tiles": sieve_ms, "search_kernel": search_ms},
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "batched": batched, "served": served,
+            "batched": batched, "served": served, "sieve_sweep": sweep,
             "gpu_launches": 2 * args.steps,
         }
         print(json.dumps(line), flush=True)
@@ -312,6 +315,46 @@ def batched_section(args, dev):
             "plain_one_launch_per_range": {"value": plain, "unit": UNIT,
                                            "sample": f"{len(sample)} of the 256 ranges (every 16th)"},
             "vs_plain": value / plain}
+
+
+# ---------------------------------------------------------------------------------------
+# sieve sweep: the map for N = 2^24, 2^28, 2^32 with the shared-memory tile swept
+# ---------------------------------------------------------------------------------------
+def sieve_sweep_section(args, dev, hbm_peak):
+    import torch
+    import ffb200 as ffb
+    lib = ffb.load()
+    stream = torch.cuda.Stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    marks = {24: 1.53e7, 28: 2.66e8, 32: 4.55e9}   # odd multiples >= p^2 of odd primes <= sqrt(N)
+    out = []
+    for logn in (24, 28, 32):
+        n = 1 << logn
+        nbytes = (n + 1 + 15) >> 4
+        d = torch.empty(nbytes + 64, dtype=torch.uint8, device="cuda")
+        row = {"N": f"2^{logn}", "map_bytes": nbytes, "tiles": {}}
+        for kb in (64, 96, 128, 160, 192, 216):
+            for _ in range(3):
+                assert lib.ffb_sieve_map_tiled_async(dev, n, d.data_ptr(), kb * 1024, sp) == 0
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            reps = 20 if logn < 32 else 5
+            e0.record(stream)
+            for _ in range(reps):
+                assert lib.ffb_sieve_map_tiled_async(dev, n, d.data_ptr(), kb * 1024, sp) == 0
+            e1.record(stream)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            gbs = nbytes / (ms / 1e3) / 1e9
+            row["tiles"][f"{kb}KB"] = {"ms": ms, "GB/s": gbs, "frac_of_hbm": gbs / hbm_peak,
+                                       "marks_per_s": marks[logn] / (ms / 1e3)}
+        best = max(row["tiles"].items(), key=lambda kv: kv[1]["GB/s"])
+        row["best"] = {"tile": best[0], **best[1]}
+        out.append(row)
+        del d
+    return {"workload": "prime map for values up to N (host prime list to sqrt N, sieve only); "
+                        "a 2^24 or 2^28 map fits in L2, so only the 2^32 line is HBM-sized; "
+                        "host launch overhead included (one call per sieve)", "rows": out}
 
 
 # ---------------------------------------------------------------------------------------
@@ -539,6 +582,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the public-call timing")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-mode section")
+    ap.add_argument("--no-sieve-sweep", action="store_true", help="skip the sieve sweep section")
     ap.add_argument("--served-requests", type=int, default=400,
                     help="requests of the seed-1 served stream to replay (0: skip)")
     ap.add_argument("--served-loads", type=lambda v: [float(x) for x in v.split(",")],

@@ -128,7 +128,7 @@ int run_search(int dev, const uint8_t* d_map, uint64_t bound, uint32_t lo, uint3
 }
 
 int run_sieve(int dev, const uint32_t* h_primes, uint32_t n, uint64_t seg_lo, uint64_t seg_hi,
-              uint8_t* d_out, cudaStream_t stream, int clear_one)
+              uint8_t* d_out, cudaStream_t stream, int clear_one, uint32_t tile_bytes)
 {
     DeviceState* s = device_state(dev);
     if (!s) return -1;
@@ -139,7 +139,7 @@ int run_sieve(int dev, const uint32_t* h_primes, uint32_t n, uint64_t seg_lo, ui
     a.seg_hi = seg_hi;
     a.h_primes = h_primes;
     a.nprimes = n;
-    a.tile_bytes = 0;
+    a.tile_bytes = tile_bytes;
     a.clear_one = clear_one;
     return launch_sieve(a, s->sms, stream);
 }
@@ -455,6 +455,22 @@ extern "C" int ffb_sieve_map_async(int deviceIndex, uint64_t mpv, uint8_t* d_map
     uint32_t n = 0;
     host_odd_primes(isqrt_u64(mpv), &pr, &n);
     int rc = run_sieve(deviceIndex, pr, n, 0, mpv + 1, d_map, (cudaStream_t)stream, 1);
+    std::free(pr);
+    return rc;
+}
+
+extern "C" int ffb_sieve_map_tiled_async(int deviceIndex, uint64_t mpv, uint8_t* d_map,
+                                         uint32_t tileBytes, void* stream)
+{
+    if (tileBytes < 1024 || tileBytes > 216 * 1024 || (tileBytes & 15)) {
+        std::fprintf(stderr, "ffb_sieve_map_tiled_async: tile of %u bytes outside 1 KB..216 KB "
+                     "(multiple of 16)\n", tileBytes);
+        return -1;
+    }
+    uint32_t* pr = nullptr;
+    uint32_t n = 0;
+    host_odd_primes(isqrt_u64(mpv), &pr, &n);
+    int rc = run_sieve(deviceIndex, pr, n, 0, mpv + 1, d_map, (cudaStream_t)stream, 1, tileBytes);
     std::free(pr);
     return rc;
 }

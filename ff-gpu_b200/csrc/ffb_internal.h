@@ -77,7 +77,7 @@ int launch_search(const SearchArgs& a, int sms, cudaStream_t stream);
 
 // Entry helpers shared by the C ABI and the pipeline (capi.cu).
 int run_sieve(int dev, const uint32_t* h_primes, uint32_t n, uint64_t seg_lo, uint64_t seg_hi,
-              uint8_t* d_out, cudaStream_t stream, int clear_one);
+              uint8_t* d_out, cudaStream_t stream, int clear_one, uint32_t tile_bytes = 0);
 int run_search(int dev, const uint8_t* d_map, uint64_t bound, uint32_t lo, uint32_t hi,
                uint64_t* d_rec, void* grec, uint32_t grec_base, uint32_t* gcount,
                cudaStream_t stream);

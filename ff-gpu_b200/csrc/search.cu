@@ -60,6 +60,18 @@ __device__ __forceinline__ bool pair1(const SearchArgs& A, uint64_t i)
     return isp<kMR>(A, i - 2);
 }
 
+// single_pair(i) as far as it is decided without Miller-Rabin: 0 false, 1 true, 2 the probe
+// i - 2 lies above the map and has no factor below 64 (Miller-Rabin decides).
+__device__ __forceinline__ int pair_class(const SearchArgs& A, uint64_t i)
+{
+    if (!(i & 1)) return 1;
+    const uint64_t n = i - 2;
+    if (n <= A.bound) return (__ldg(A.map + (n >> 4)) >> (7 - ((n >> 1) & 7))) & 1;
+    if (n >= (1ull << 48)) atomicOr(A.err, kErrMrDomain);
+    if (n > 61 && small_factor(n)) return 0;
+    return 2;
+}
+
 // Ascending prime factorisation of an odd x < 2^32 by the exact-division table, with the
 // cofactor's primality read from the bitmap after every factor found.
 template <bool kMR>
@@ -179,6 +191,85 @@ __device__ __noinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const
     return nm == 1;
 }
 
+// all_but_one for the Miller-Rabin variant: the same divisor pairs in the same order, but a
+// pair sum whose probe lies above the map (and has no small factor) is appended to pend[]
+// instead of being tested here, so that the warp can test them 32 at a time. Returns the
+// count of pairs already known not to be single (2 once the verdict is "no"); the verdict is
+// "yes" iff that count plus the pending probes found composite is exactly 1 (the order of the
+// tests does not change it). *np receives the number of pending pair sums.
+__device__ __noinline__ uint32_t all_but_one_defer(uint32_t k, uint64_t odd_product, const Fac& f,
+                                                   const SearchArgs& A, uint64_t* pend,
+                                                   uint32_t* np)
+{
+    const uint64_t P = odd_product << k;
+    const uint64_t lim = isqrt64(P);
+    uint64_t F[kMaxDiv], C[kMaxDiv];
+    uint32_t nf = 0, npend = 0, nm = 0, nd = 0;
+    *np = 0;
+    // counts a pair sum: 0 not single, 1 single, 2 pending; returns true once nm > 1
+    auto visit = [&](uint64_t v) {
+        const int c = pair_class(A, v);
+        if (c == 2) pend[nd++] = v;
+        else nm += c == 0;
+        return nm > 1;
+    };
+    F[0] = 1ull << k;
+    C[0] = odd_product;
+    if (F[0] <= lim) {
+        visit(F[0] + C[0]);
+        nf = 1;
+    }
+    int idx = 0;
+    bool first = true;  // the reference tries 3 before its first IsPrime(testProduct)
+    for (;;) {
+        uint64_t q;
+        uint32_t e;
+        if (first) {
+            first = false;
+            if (f.n > 0 && f.q[0] == 3) { q = 3; e = f.e[0]; idx = 1; }
+            else continue;
+        } else {
+            if (idx >= f.n) break;                                   // testProduct == 1
+            q = f.q[idx];
+            e = f.e[idx];
+            if (idx == f.n - 1 && e == 1 && q > lim) break;          // prime cofactor > limit
+            ++idx;
+        }
+        const uint64_t qi = inv64(q);
+        uint64_t tf = q, tfi = qi;
+        for (uint32_t j = 0; j < e; ++j) {
+            if (tf <= lim) {
+                const uint64_t ctf = (odd_product * tfi) << k;     // P / tf, exact
+                if (visit(tf + ctf)) return 2;
+                if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return 2; }
+                F[nf + npend] = tf;
+                C[nf + npend] = ctf;
+                ++npend;
+                for (uint32_t g = 0; g < nf; ++g) {
+                    const uint64_t m = F[g] * tf;
+                    if (m <= lim) {
+                        const uint64_t cm = C[g] * tfi;              // C[g] / tf, exact
+                        if (visit(m + cm)) return 2;
+                        if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return 2; }
+                        F[nf + npend] = m;
+                        C[nf + npend] = cm;
+                        ++npend;
+                    } else {
+                        // skip the rest of this ascending run of F (reference :451)
+                        for (const uint64_t v = F[g]; g + 1 < nf && v <= F[g + 1]; ++g) {}
+                    }
+                }
+            }
+            tf *= q;
+            tfi *= qi;
+        }
+        nf += npend;
+        npend = 0;
+    }
+    *np = nd;
+    return nm;
+}
+
 // Split encoding in the queues: bits 0..4 k, bit 5 composite (Power2Composite item: the odd
 // term is sum - 2^k), bits 6..31 the odd part o of the even term (o < 2^26).
 __device__ __forceinline__ uint32_t enc(uint32_t k, uint32_t o, bool comp)
@@ -210,6 +301,31 @@ __device__ bool stage2(uint32_t item, uint32_t s, const SearchArgs& A, uint32_t*
     return all_but_one<kMR>(k, odd_product, f, A);
 }
 
+// Stage 2 of the Miller-Rabin variant: the factorisation and the divisor pairs, with the
+// pair probes above the map left in pend[] (see all_but_one_defer).
+__device__ uint32_t stage2_defer(uint32_t item, uint32_t s, const SearchArgs& A, uint32_t* ta,
+                                 uint32_t* tb, uint64_t* pend, uint32_t* np)
+{
+    const uint32_t k = item & 31;
+    Fac f;
+    uint64_t odd_product;
+    if (item & 32) {
+        const uint32_t odd = s - (1u << k);
+        factor_product<true>(odd, 1, f, A);
+        odd_product = odd;
+        *ta = 1u << k;
+        *tb = odd;
+    } else {
+        const uint32_t o = item >> 6;
+        const uint32_t even = o << k, b = s - even;
+        factor_product<true>(o, b, f, A);
+        odd_product = (uint64_t)o * b;
+        *ta = even;
+        *tb = b;
+    }
+    return all_but_one_defer(k, odd_product, f, A, pend, np);
+}
+
 // Stage 1: the pair sum 2^k + o*b whose probe 2^k + o*b - 2 is DoesPeterKnow's first test.
 __device__ __forceinline__ uint64_t stage1_value(uint32_t item, uint32_t s)
 {
@@ -230,6 +346,7 @@ struct WarpQ {
     uint32_t a[kCap];
     uint32_t b[kCap];
     uint32_t c[kMR ? kCap : 1];
+    uint64_t probe[kMR ? 32 : 1];  // stage-2 probes handed to the warp's Miller-Rabin
 };
 
 // Appends the items of the lanes with `pred` to q[n..]; returns the new size (uniform).
@@ -247,18 +364,6 @@ struct SumState {
     uint32_t ta, tb;      // terms of the first valid split
     uint32_t na, nb, nc;  // queue sizes
 };
-
-// single_pair(i) as far as it is decided without Miller-Rabin: 0 false, 1 true, 2 the probe
-// i - 2 lies above the map and has no factor below 64 (Miller-Rabin decides).
-__device__ __forceinline__ int pair_class(const SearchArgs& A, uint64_t i)
-{
-    if (!(i & 1)) return 1;
-    const uint64_t n = i - 2;
-    if (n <= A.bound) return (__ldg(A.map + (n >> 4)) >> (7 - ((n >> 1) & 7))) & 1;
-    if (n >= (1ull << 48)) atomicOr(A.err, kErrMrDomain);
-    if (n > 61 && small_factor(n)) return 0;
-    return 2;
-}
 
 // Runs stage 1 on up to 32 queued items: passes go to queue b; with the Miller-Rabin variant,
 // probes above the map go to queue c.
@@ -320,7 +425,44 @@ __device__ void drain_b(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int la
     __syncwarp();
     st.nb = base;
     uint32_t a = 0, b = 0;
-    const bool valid = act && stage2<kMR>(item, st.s, A, &a, &b);
+    bool valid;
+    if constexpr (kMR) {
+        uint64_t pend[kMaxDiv];
+        uint32_t np = 0;
+        uint32_t nm = act ? stage2_defer(item, st.s, A, &a, &b, pend, &np) : 2;
+        // the pending pair probes of all lanes, packed 32 to a Miller-Rabin round: each lane
+        // fills the slots [excl, excl + take) of the staging area with its next probes, and
+        // counts the composites among them
+        uint32_t next = 0;
+        for (;;) {
+            const uint32_t rem = nm <= 1 ? np - next : 0;
+            uint32_t incl = rem;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+                if (lane >= d) incl += t;
+            }
+            const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+            if (total == 0) break;
+            const uint32_t excl = incl - rem;
+            const uint32_t take = excl < 32 ? (rem < 32 - excl ? rem : 32 - excl) : 0;
+            for (uint32_t i = 0; i < take; ++i) Q.probe[excl + i] = pend[next + i] - 2;
+            __syncwarp();
+            const bool need = (uint32_t)lane < (total < 32 ? total : 32);
+            const uint64_t n = need ? Q.probe[lane] : 0;
+            __syncwarp();
+            const bool prime = mr_rounds(n, need, lane, lane == 0 ? A.stats : nullptr);
+            const uint32_t comp = __ballot_sync(0xFFFFFFFFu, need && !prime);
+            if (take) {
+                const uint32_t mine = take == 32 ? 0xFFFFFFFFu : ((1u << take) - 1) << excl;
+                nm += __popc(comp & mine);
+            }
+            next += take;
+        }
+        valid = act && nm == 1;
+    } else {
+        valid = act && stage2<kMR>(item, st.s, A, &a, &b);
+    }
     const uint32_t m = __ballot_sync(0xFFFFFFFFu, valid);
     if (m) {
         const int src = __ffs(m) - 1;

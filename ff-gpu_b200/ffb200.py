@@ -118,6 +118,8 @@ SIGNATURES = {
                                     ctypes.c_uint32, u32p, u32p, ctypes.c_int]),
     "ffb_sieve_map_async": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_void_p,
                                            ctypes.c_void_p]),
+    "ffb_sieve_map_tiled_async": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_void_p,
+                                                 ctypes.c_uint32, ctypes.c_void_p]),
     "ffb_search_async": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
                                         ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
                                         ctypes.c_void_p]),

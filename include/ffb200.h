@@ -194,6 +194,12 @@ int ffb_schedule(uint32_t sumStart, uint32_t sumLimit, uint64_t maxPrimeMapValue
 int ffb_sieve_map_async(int deviceIndex, uint64_t maxPrimeMapValue, uint8_t* d_map,
                         void* stream);
 
+/* ffb_sieve_map_async with the shared-memory tile of the sieve given (1 KB..216 KB, a
+ * multiple of 16; the default is 96 KB): the slab-size knob of the reference's engine
+ * (--slab-size), for sweeps and tuning. */
+int ffb_sieve_map_tiled_async(int deviceIndex, uint64_t maxPrimeMapValue, uint8_t* d_map,
+                              uint32_t tileBytes, void* stream);
+
 /* Packed search results for the odd sums lo..hi (lo, hi odd): d_rec[(s-lo)/2] = 0 or
  * (low | lowPrime<<31) << 32 | (high | highPrime<<31). Values <= mapBound are answered by
  * d_map, larger ones by Miller-Rabin. d_rec is zero-filled by the call. Stream-ordered. */
@@ -319,7 +325,7 @@ typedef struct {
     uint32_t launchWork;        /* work of one launch in odd sums at sum 2^21 (a sum s counts
                                    s/2^21); 0 = 65536 */
     uint32_t launchSums;        /* most odd sums of one launch; 0 = 2^22 */
-    uint32_t searchWarps;       /* warps per search block: 4, 8 or 16; 0 = 16 */
+    uint32_t searchWarps;       /* warps per search block: 4, 8 or 16; 0 = 4 */
     uint32_t warmLimit;         /* sieve the map for sums up to this at creation; 0 = none */
 } FfbServeConfig;
 typedef struct {

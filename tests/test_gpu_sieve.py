@@ -96,6 +96,25 @@ def test_sieve_sweep_prime_counts(ffb, oracle, logn, pi):
             assert np.array_equal(got[: len(want) - 1], want[:-1])
 
 
+@pytest.mark.parametrize("tile_kb", [64, 96, 128, 160, 192, 216])
+def test_sieve_tile_sizes_give_the_same_map(ffb, oracle, tile_kb):
+    """The C3 sweep's tile sizes (ffb_sieve_map_tiled_async): every tile gives the map of the
+    literal fill (2^28) and the exact prime count."""
+    import torch
+    n = 1 << 28
+    d = torch.empty(((n + 1 + 15) >> 4) + 16, dtype=torch.uint8, device="cuda")
+    assert ffb.load().ffb_sieve_map_tiled_async(0, n, d.data_ptr(), tile_kb * 1024, None) == 0
+    torch.cuda.synchronize()
+    assert prime_count_below(d, n) == 14630843
+    assert np.array_equal(d[: (n + 16) >> 4].cpu().numpy(), oracle.build_map(n))
+
+
+def test_sieve_tile_size_limits(ffb):
+    lib = ffb.load()
+    assert lib.ffb_sieve_map_tiled_async(0, 1 << 20, None, 217 * 1024, None) == -1
+    assert lib.ffb_sieve_map_tiled_async(0, 1 << 20, None, 1000, None) == -1
+
+
 def test_pool_ops_and_semantics(ffb, oracle):
     """slabCompute(primeSlab=0) clears bits INTO whatever the slab holds, like the reference."""
     lib = ffb.load()
