@@ -497,21 +497,37 @@ __device__ __forceinline__ bool settle(SumState& st, WarpQ<kMR>& Q, const Search
 // of DoesPeterKnow (:636): o == b or o + b*2^k - 2 prime. Returns 0 rejected, 1 passed,
 // 2 the probe waits for Miller-Rabin (only when kMR).
 template <bool kOdd, bool kMR>
-__device__ __forceinline__ int stage0(uint32_t s, uint32_t k, uint32_t o, const SearchArgs& A)
+__device__ __forceinline__ int stage0(uint32_t s, uint32_t k, uint32_t o, bool act,
+                                      const SearchArgs& A)
 {
-    const uint32_t b = s - (o << k);
-    const bool pre = kOdd ? (o % 3 != 0 && b % 3 != 0)
-                          : (o % 3 == 0 || b % 3 == 0 || isp<kMR>(A, b));
-    if (!pre) return 0;
-    if (o == b) return 1;
+    // Both map reads are issued before any branch (the probe is clamped into the map, and
+    // b is only read for an active lane), so the two splits a lane holds per step overlap
+    // their latency. b = s - o*2^k is odd and below s; v = o + b*2^k is odd, so the probe of
+    // single_pair(v) is v - 2.
+    const uint32_t b = act ? s - (o << k) : 1;
     const uint64_t v = o + ((uint64_t)b << k);
-    if (kMR) return pair_class(A, v);
-    return pair1<kMR>(A, v) ? 1 : 0;
+    const uint64_t n = v - 2;
+    const uint64_t nr = n <= A.bound ? n : 1;
+    const uint32_t mv = __ldg(A.map + (nr >> 4));
+    bool pre;
+    if (kOdd) {
+        pre = o % 3 != 0 && b % 3 != 0;
+    } else {
+        const uint32_t mb = __ldg(A.map + (b >> 4));
+        pre = o % 3 == 0 || b % 3 == 0 || ((mb >> (7 - ((b >> 1) & 7))) & 1);
+    }
+    if (!act || !pre) return 0;
+    if (o == b) return 1;
+    if (n > A.bound) {
+        if constexpr (kMR) return pair_class(A, v);
+        else return miller_rabin_plain(n, A.err) ? 1 : 0;
+    }
+    return (mv >> (7 - ((n >> 1) & 7))) & 1;
 }
 
 // Enumerates the splits of one phase for sum s: k = kfirst, kfirst+2, ... while o0<<k < s-2;
-// for each k the odd parts o = o0, o0+2, ... with o<<k < s-2. Returns false once the sum
-// is rejected (two valid splits).
+// for each k the odd parts o = o0, o0+2, ... with o<<k < s-2, two per lane per step. Returns
+// false once the sum is rejected (two valid splits).
 template <bool kOdd, bool kMR>
 __device__ bool run_phase(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int lane)
 {
@@ -521,19 +537,25 @@ __device__ bool run_phase(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int 
         // odd o in [o0, omax] with o<<k <= s-3
         const uint32_t omax = (s - 3) >> k;
         const uint32_t n = omax >= o0 ? ((omax - o0) >> 1) + 1 : 0;
-        for (uint32_t base = 0; base < n; base += 32) {
-            const uint32_t i = base + lane;
-            const uint32_t o = o0 + 2 * i;
-            const int cls = i < n ? stage0<kOdd, kMR>(s, k, o, A) : 0;
-            st.na = push(Q.a, st.na, cls == 1, enc(k, o, false), lane);
-            if constexpr (kMR) {
-                st.nc = push(Q.c, st.nc, cls == 2, enc(k, o, true), lane);
-                if (!settle(st, Q, A, lane)) return false;
-            } else if (st.na >= 32) {
-                drain_a(st, Q, A, lane);
-                if (st.nb >= 32) {
-                    drain_b(st, Q, A, lane);
-                    if (st.count > 1) return false;
+        for (uint32_t base = 0; base < n; base += 64) {
+            const uint32_t i0 = base + lane, i1 = i0 + 32;
+            const uint32_t oa = o0 + 2 * i0, ob = o0 + 2 * i1;
+            const int ca = stage0<kOdd, kMR>(s, k, oa, i0 < n, A);
+            const int cb = stage0<kOdd, kMR>(s, k, ob, i1 < n, A);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int cls = h ? cb : ca;
+                const uint32_t o = h ? ob : oa;
+                st.na = push(Q.a, st.na, cls == 1, enc(k, o, false), lane);
+                if constexpr (kMR) {
+                    st.nc = push(Q.c, st.nc, cls == 2, enc(k, o, true), lane);
+                    if (!settle(st, Q, A, lane)) return false;
+                } else if (st.na >= 32) {
+                    drain_a(st, Q, A, lane);
+                    if (st.nb >= 32) {
+                        drain_b(st, Q, A, lane);
+                        if (st.count > 1) return false;
+                    }
                 }
             }
         }
