@@ -37,17 +37,19 @@ struct Fac {
     int n;
 };
 
-// Prime::IsPrime for the search (reference/segmentedSieve.C:283-296). The map-only
-// variant is launched only when the map reaches every value the search can ask about; its
-// Miller-Rabin is the plain form, which it never reaches.
+// Prime::IsPrime for the search (reference/segmentedSieve.C:283-296), for the values that
+// are (almost) always in the map: terms below the sum, cofactors below 2^32. The map-only
+// variant is launched only when the map reaches every value the search can ask about, and
+// the probes that can leave the map in the Miller-Rabin variant go through pair_class and
+// the batched test instead; so the per-lane Miller-Rabin here is the plain form, which
+// keeps the register allocation of both kernels at their best measured.
 template <bool kMR>
 __device__ __forceinline__ bool isp(const SearchArgs& A, uint64_t n)
 {
     if (n == 2) return true;
     if (!(n & 1)) return false;
     if (n > A.bound) {
-        if constexpr (kMR) return miller_rabin(n, A.err);
-        else return miller_rabin_plain(n, A.err);
+        return miller_rabin_plain(n, A.err);
     }
     return (__ldg(A.map + (n >> 4)) >> (7 - ((n >> 1) & 7))) & 1;
 }
@@ -381,7 +383,7 @@ __device__ void drain_a(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int la
     if (kMR) {
         const int cls = act ? pair_class(A, v) : 0;
         st.nb = push(Q.b, st.nb, cls == 1, item, lane);
-        st.nc = push(Q.c, st.nc, cls == 2, item, lane);
+        if (__any_sync(0xFFFFFFFFu, cls == 2)) st.nc = push(Q.c, st.nc, cls == 2, item, lane);
     } else {
         const bool pass = act && pair1<kMR>(A, v);
         st.nb = push(Q.b, st.nb, pass, item, lane);
@@ -548,8 +550,9 @@ __device__ bool run_phase(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int 
                 const uint32_t o = h ? ob : oa;
                 st.na = push(Q.a, st.na, cls == 1, enc(k, o, false), lane);
                 if constexpr (kMR) {
-                    st.nc = push(Q.c, st.nc, cls == 2, enc(k, o, true), lane);
-                    if (!settle(st, Q, A, lane)) return false;
+                    if (__any_sync(0xFFFFFFFFu, cls == 2))
+                        st.nc = push(Q.c, st.nc, cls == 2, enc(k, o, true), lane);
+                    if ((st.na >= 32 || st.nc >= 32) && !settle(st, Q, A, lane)) return false;
                 } else if (st.na >= 32) {
                     drain_a(st, Q, A, lane);
                     if (st.nb >= 32) {
