@@ -160,22 +160,11 @@ __device__ __forceinline__ bool small_factor(uint64_t n)
 }
 
 // Miller-Rabin with the reference's bases and thresholds (reference/segmentedSieve.C:
-// 365-389) for one lane. For odd n in [17, 2^48) the verdicts equal the reference's (its
-// software mulmod is exact there); the small-prime test in front only removes composites.
-static __device__ __noinline__ bool miller_rabin(uint64_t n, uint32_t* err)
-{
-    if (n >= (1ull << 48)) atomicOr(err, kErrMrDomain);
-    if (n > 61 && small_factor(n)) return false;
-    const uint32_t tests = mr_tests(n);
-    for (uint32_t i = 0; i < tests; ++i)
-        if (!sprp(n, mr_base(i))) return false;
-    return true;
-}
-
-// The same Miller-Rabin written plainly (64-bit remainders in the set-up, no small-prime
-// test, base by base). It is the fallback of the map-only search, where no value reaches
-// it: in that kernel this form of the callee measured fastest (its calls shape the
-// kernel's register allocation even when never taken).
+// 365-389) for one lane, written plainly (64-bit remainders in the set-up, base by base).
+// For odd n in [17, 2^48) the verdicts equal the reference's (its software mulmod is exact
+// there). The search calls it only for values that are almost never above the map; the
+// probes that do leave the map are tested in batches (mr_rounds). This form of the callee
+// measured fastest: its calls shape the kernels' register allocation even when not taken.
 static __device__ __noinline__ bool miller_rabin_plain(uint64_t n, uint32_t* err)
 {
     if (n >= (1ull << 48)) atomicOr(err, kErrMrDomain);
@@ -252,26 +241,5 @@ __device__ __forceinline__ bool mr_rounds(uint64_t n, bool need, int lane,
     }
     return pp && !((fail >> lane) & 1);
 }
-
-// Prime::IsPrime (reference/segmentedSieve.C:283-296): 2 -> prime, even -> not, above the
-// map -> Miller-Rabin, else the map bit.
-__device__ __forceinline__ bool is_prime(const uint8_t* __restrict__ map, uint64_t bound,
-                                         uint64_t n, uint32_t* err)
-{
-    if (n == 2) return true;
-    if (!(n & 1)) return false;
-    if (n > bound) return miller_rabin(n, err);
-    return (__ldg(map + (n >> 4)) >> (7 - ((n >> 1) & 7))) & 1;
-}
-
-// ProductOfTermPairsHasSingleFactorPair (reference/segmentedSieve.C:419-422): an even pair
-// sum always has a prime split (Goldbach); an odd one has only 2 + (i-2).
-__device__ __forceinline__ bool single_pair(const uint8_t* __restrict__ map, uint64_t bound,
-                                            uint64_t i, uint32_t* err)
-{
-    if (!(i & 1)) return true;
-    return is_prime(map, bound, i - 2, err);
-}
-
 
 }  // namespace ffb
