@@ -121,6 +121,8 @@ def ours(args, rank, world, dist):
     # the output is the same either way, Miller-Rabin being exact)
     gs = geometry_for(ffb, b + 1)
     mpv = max(gs.maxPrimeMapValue, lib.ffb_probe_bound(b))
+    if args.map_bound:          # a smaller map: probes above it go to the Miller-Rabin variant
+        mpv = min(mpv, (args.map_bound + 1) // 16 * 16 - 1)
     nsums = odd_sums(a, b)
     d_map = torch.empty(((mpv + 1 + 15) >> 4) + 64, dtype=torch.uint8, device="cuda")
     d_rec = torch.empty(max(nsums, 1), dtype=torch.int64, device="cuda")
@@ -583,12 +585,15 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the public-call timing")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-mode section")
     ap.add_argument("--no-sieve-sweep", action="store_true", help="skip the sieve sweep section")
-    ap.add_argument("--served-requests", type=int, default=400,
+    ap.add_argument("--served-requests", type=int, default=300,
                     help="requests of the seed-1 served stream to replay (0: skip)")
     ap.add_argument("--served-loads", type=lambda v: [float(x) for x in v.split(",")],
                     default=[0.5, 0.8], help="offered loads, as fractions of the measured capacity")
     ap.add_argument("--served-plain", type=int, default=8,
                     help="requests timed through the plain method for the comparison")
+    ap.add_argument("--map-bound", type=int, default=0,
+                    help="cap the map at this value (probes above it take the Miller-Rabin "
+                         "search variant); 0 = the bound covering every probe")
     ap.add_argument("--limit", type=int, default=2097152,
                     help="sumLimit of the job (2^21 for the reported line; smaller for profiling)")
     args = ap.parse_args()
