@@ -339,7 +339,7 @@ __device__ __forceinline__ uint64_t stage1_value(uint32_t item, uint32_t s)
 // Per-warp queues of pending split items (shared memory). With the Miller-Rabin variant
 // a third queue holds the items whose probe lies above the map and survived the small-prime
 // test, so that Miller-Rabin always runs on 32 candidates at once. Each queue holds at most
-// 127 items: before any stage pushes, every queue holds fewer than 32 (settle() below),
+// 127 items: before any stage pushes, every queue holds fewer than 32 (settle_mr below),
 // a stage pushes at most 32 items in all, and a drain never outputs more than it takes,
 // so the total stays below 128.
 template <bool kMR>
@@ -475,18 +475,21 @@ __device__ void drain_b(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int la
     }
 }
 
-// Drains every queue that holds 32 or more items (b first: it may reject the sum and pushes
-// nothing). Returns false once the sum is rejected.
-template <bool kMR>
-__device__ __forceinline__ bool settle(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int lane)
+// The Miller-Rabin variant's queue work in one non-inlined routine (all 32 lanes call it
+// together), so each drain's code exists once: that kernel is otherwise large enough to
+// stall on instruction fetch. Drains every queue that holds 32 or more items (b first: it
+// may reject the sum and pushes nothing); with `flush`, also the partly filled ones, until
+// all are empty. Returns false once the sum is rejected.
+__device__ __noinline__ bool settle_mr(SumState& st, WarpQ<true>& Q, const SearchArgs& A,
+                                       int lane, bool flush)
 {
     for (;;) {
-        if (st.nb >= 32) {
+        if (st.nb >= 32 || (flush && st.nb > 0 && st.na == 0 && st.nc == 0)) {
             drain_b(st, Q, A, lane);
             if (st.count > 1) return false;
-        } else if (kMR && st.nc >= 32) {
+        } else if (st.nc >= 32 || (flush && st.nc > 0 && st.na == 0)) {
             drain_c(st, Q, A, lane);
-        } else if (st.na >= 32) {
+        } else if (st.na >= 32 || (flush && st.na > 0)) {
             drain_a(st, Q, A, lane);
         } else {
             return true;
@@ -552,7 +555,8 @@ __device__ bool run_phase(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int 
                 if constexpr (kMR) {
                     if (__any_sync(0xFFFFFFFFu, cls == 2))
                         st.nc = push(Q.c, st.nc, cls == 2, enc(k, o, true), lane);
-                    if ((st.na >= 32 || st.nc >= 32) && !settle(st, Q, A, lane)) return false;
+                    if ((st.na >= 32 || st.nc >= 32) && !settle_mr(st, Q, A, lane, false))
+                        return false;
                 } else if (st.na >= 32) {
                     drain_a(st, Q, A, lane);
                     if (st.nb >= 32) {
@@ -666,18 +670,17 @@ __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
             // Power2Composite items (reference/segmentedSieve.C:591-605) go straight to stage 2
             st.nb = push(Q.b, 0, (cmask >> lane) & 1, enc(lane, 0, true), lane);
             bool open = true;
-            if (st.nb >= 32) { drain_b(st, Q, A, lane); open = st.count <= 1; }
+            if constexpr (kMR) {
+                if (st.nb >= 32) open = settle_mr(st, Q, A, lane, false);
+            } else if (st.nb >= 32) {
+                drain_b(st, Q, A, lane);
+                open = st.count <= 1;
+            }
             if (open) open = run_phase<true, kMR>(st, Q, A, lane);
             if (open) open = run_phase<false, kMR>(st, Q, A, lane);
             // flush the partly filled queues: stage 1, then Miller-Rabin, then stage 2
             if constexpr (kMR) {
-                while (open) {
-                    if (st.na > 0) drain_a(st, Q, A, lane);
-                    else if (st.nc > 0) drain_c(st, Q, A, lane);
-                    else if (st.nb > 0) drain_b(st, Q, A, lane);
-                    else break;
-                    open = st.count <= 1 && settle(st, Q, A, lane);
-                }
+                if (open) open = settle_mr(st, Q, A, lane, true);
             } else {
                 while (open && st.na > 0) {
                     drain_a(st, Q, A, lane);
