@@ -207,9 +207,9 @@ static __device__ __noinline__ bool miller_rabin_plain(uint64_t n, uint32_t* err
 static __device__ __noinline__ bool sprp_leaf(uint64_t n, uint32_t b) { return sprp(n, b); }
 
 // Miller-Rabin rounds for the lanes with `need` (odd candidates without small factors), all
-// 32 lanes calling together. cnt (non-null on one lane only) counts [2] candidates and
+// 32 lanes calling together; one out-of-line copy keeps the calling kernel's code small. cnt (non-null on one lane only) counts [2] candidates and
 // [3] base-2 survivors.
-__device__ __forceinline__ bool mr_rounds(uint64_t n, bool need, int lane,
+static __device__ __noinline__ bool mr_rounds(uint64_t n, bool need, int lane,
                                           unsigned long long* cnt)
 {
     const uint32_t want = __ballot_sync(0xFFFFFFFFu, need);

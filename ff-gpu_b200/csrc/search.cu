@@ -62,6 +62,14 @@ __device__ __forceinline__ bool pair1(const SearchArgs& A, uint64_t i)
     return isp<kMR>(A, i - 2);
 }
 
+// A probe above the map: 0 when it has an odd prime factor below 64 (composite), else 2
+// (Miller-Rabin decides). Out of line: several call sites, taken only above the map.
+__device__ __noinline__ int above_map_class(uint64_t n, uint32_t* err)
+{
+    if (n >= (1ull << 48)) atomicOr(err, kErrMrDomain);
+    return n > 61 && small_factor(n) ? 0 : 2;
+}
+
 // single_pair(i) as far as it is decided without Miller-Rabin: 0 false, 1 true, 2 the probe
 // i - 2 lies above the map and has no factor below 64 (Miller-Rabin decides).
 __device__ __forceinline__ int pair_class(const SearchArgs& A, uint64_t i)
@@ -69,9 +77,7 @@ __device__ __forceinline__ int pair_class(const SearchArgs& A, uint64_t i)
     if (!(i & 1)) return 1;
     const uint64_t n = i - 2;
     if (n <= A.bound) return (__ldg(A.map + (n >> 4)) >> (7 - ((n >> 1) & 7))) & 1;
-    if (n >= (1ull << 48)) atomicOr(A.err, kErrMrDomain);
-    if (n > 61 && small_factor(n)) return 0;
-    return 2;
+    return above_map_class(n, A.err);
 }
 
 // Ascending prime factorisation of an odd x < 2^32 by the exact-division table, with the

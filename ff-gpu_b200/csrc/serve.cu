@@ -524,7 +524,7 @@ extern "C" FfbServer* ffb_serve_create(int deviceIndex, const FfbServeConfig* cf
     c.slots = std::min<uint32_t>(c.slots, kMaxSlots);
     if (c.launchWork == 0) c.launchWork = 65536;
     if (c.launchSums == 0) c.launchSums = 1u << 22;
-    if (c.searchWarps != 8 && c.searchWarps != 16) c.searchWarps = 4;  // fastest measured
+    if (c.searchWarps != 4 && c.searchWarps != 16) c.searchWarps = 8;  // fastest measured
     size_t free_b = 0, total_b = 0;
     if (cudaSetDevice(deviceIndex) != cudaSuccess || cudaMemGetInfo(&free_b, &total_b) != cudaSuccess ||
         ffb_compute_budget(free_b, c.vramFraction, c.vramBudgetBytes, 0, 0, &S->budget)) {

@@ -325,7 +325,7 @@ typedef struct {
     uint32_t launchWork;        /* work of one launch in odd sums at sum 2^21 (a sum s counts
                                    s/2^21); 0 = 65536 */
     uint32_t launchSums;        /* most odd sums of one launch; 0 = 2^22 */
-    uint32_t searchWarps;       /* warps per search block: 4, 8 or 16; 0 = 4 */
+    uint32_t searchWarps;       /* warps per search block: 4, 8 or 16; 0 = 8 */
     uint32_t warmLimit;         /* sieve the map for sums up to this at creation; 0 = none */
 } FfbServeConfig;
 typedef struct {
