@@ -432,6 +432,11 @@ def served_section(args, dev):
     # capacity: the whole prefix at once
     sat = serve_stream(ffb, dev, [(0.0, a, b) for _, a, b in base], budget)
     cap_rps = sat["requests_per_s"]
+    # the same at a budget whose backing holds every probe of sums up to 2^22 (no
+    # Miller-Rabin): what the 8 GiB cap costs
+    full_budget = (((lib.ffb_probe_bound(1 << 22) + 1) >> 4) + (1 << 20) + (1 << 30) + (64 << 20))
+    full_budget = (full_budget + (1 << 30) - 1) >> 30 << 30
+    sat_full = serve_stream(ffb, dev, [(0.0, a, b) for _, a, b in base], full_budget)
     runs = []
     for frac in args.served_loads:
         rate = frac * cap_rps
@@ -443,7 +448,8 @@ def served_section(args, dev):
         runs.append(r)
     # the plain method once per request (ffb_run: its own map sieved, then the search)
     ctx = lib.ffb_context_create(dev)
-    sample = base[::max(1, n // args.served_plain)]
+    k = max(1, n // args.served_plain)
+    sample = base[k // 2::k]
     p, m = ctypes.c_void_p(), ctypes.c_size_t()
     plain_t, plain_sums, plain_lat = 0.0, 0, []
     try:
@@ -462,16 +468,26 @@ def served_section(args, dev):
                               if (f | 1) <= l)
     finally:
         lib.ffb_context_destroy(ctx)
-    plain = plain_sums / plain_t
+    # the plain method's time for the whole mix, estimated from the sample by request count
+    # (each request pays its own sieve, so time is not proportional to sums): the sample is
+    # every k-th request in arrival order, unbiased for the per-request mean time
+    plain_total_s = plain_t * len(base) / len(sample)
+    plain = sat["sums"] / plain_total_s
+    sat_full_vs_plain = sat_full["value"] / plain
     return {"workload": f"first {n} of the 10,000 seed-1 requests (limit U{{69..2^22}}, "
                         f"length floor(2^U[6,20]), start max(5, limit-length+1)); Poisson "
                         f"arrivals of the seed-1 stream rescaled to each rate",
             "budget": "8 GiB (computeBudget: f 0.90, cap 8 GiB)",
             "saturation": sat, "rates": runs,
+            "saturation_full_map": {**{k: sat_full[k] for k in (
+                "value", "requests_per_s", "span_s", "latency_ms", "map_bytes", "map_max_value",
+                "budget_bytes", "mr_candidates")}},
             "plain_one_launch_per_request": {
                 "value": plain, "unit": UNIT, "latency_ms_p50": pct(plain_lat, 0.5),
-                "sample": f"{len(sample)} of the {n} requests, one ffb_run each"},
-            "vs_plain": sat["value"] / plain}
+                "est_total_s": plain_total_s, "sample_sums_per_s": plain_sums / plain_t,
+                "sample": f"every {n // len(sample)}th of the {n} requests ({len(sample)}), one "
+                          f"ffb_run each; the mix's time = mean time per request x {n}"},
+            "vs_plain": sat["value"] / plain, "full_map_vs_plain": sat_full_vs_plain}
 
 
 # ---------------------------------------------------------------------------------------
@@ -589,7 +605,7 @@ def main():
                     help="requests of the seed-1 served stream to replay (0: skip)")
     ap.add_argument("--served-loads", type=lambda v: [float(x) for x in v.split(",")],
                     default=[0.5, 0.8], help="offered loads, as fractions of the measured capacity")
-    ap.add_argument("--served-plain", type=int, default=8,
+    ap.add_argument("--served-plain", type=int, default=16,
                     help="requests timed through the plain method for the comparison")
     ap.add_argument("--map-bound", type=int, default=0,
                     help="cap the map at this value (probes above it take the Miller-Rabin "
