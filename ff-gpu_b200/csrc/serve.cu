@@ -520,9 +520,9 @@ extern "C" FfbServer* ffb_serve_create(int deviceIndex, const FfbServeConfig* cf
     if (cfg) S->cfg = *cfg;
     FfbServeConfig& c = S->cfg;
     if (!(c.vramFraction > 0)) c.vramFraction = 0.90;
-    if (c.slots == 0) c.slots = 3;
+    if (c.slots == 0) c.slots = 4;
     c.slots = std::min<uint32_t>(c.slots, kMaxSlots);
-    if (c.launchWork == 0) c.launchWork = 65536;
+    if (c.launchWork == 0) c.launchWork = 131072;  // smaller launches leave SMs idle
     if (c.launchSums == 0) c.launchSums = 1u << 22;
     if (c.searchWarps != 4 && c.searchWarps != 16) c.searchWarps = 8;  // fastest measured
     size_t free_b = 0, total_b = 0;

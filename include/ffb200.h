@@ -321,9 +321,9 @@ typedef struct FfbServer FfbServer;
 typedef struct {
     uint64_t vramBudgetBytes;   /* budget cap (the reference's --vram-budget); 0 = none */
     double vramFraction;        /* f of the free device memory; 0 = 0.90 */
-    uint32_t slots;             /* launches in flight; 0 = 3 */
+    uint32_t slots;             /* launches in flight; 0 = 4 */
     uint32_t launchWork;        /* work of one launch in odd sums at sum 2^21 (a sum s counts
-                                   s/2^21); 0 = 65536 */
+                                   s/2^21); 0 = 131072 */
     uint32_t launchSums;        /* most odd sums of one launch; 0 = 2^22 */
     uint32_t searchWarps;       /* warps per search block: 4, 8 or 16; 0 = 8 */
     uint32_t warmLimit;         /* sieve the map for sums up to this at creation; 0 = none */
