@@ -273,3 +273,52 @@ extern "C" int ffb_emit(int nargs, int32_t a1, int32_t a2, const uint64_t* h_rec
     *len = n;
     return 0;
 }
+
+extern "C" int ffb_map_dump(int deviceIndex, int nargs, int32_t a1, int32_t a2, uint8_t** map,
+                            uint64_t* bytes, char* hdr, size_t hdrCap)
+{
+    if (!map || !bytes) return -1;
+    *map = nullptr;
+    *bytes = 0;
+    uint32_t start, limit;
+    parse_args(nargs, a1, a2, &start, &limit);
+    char h[2048];
+    Geometry g;
+    const int hn = plan_geometry(start, limit, &g, h, sizeof h);
+    if (hn < 0) {
+        std::fprintf(stderr, "ffb_map_dump: %s", g.too_big ? h : "header overflow\n");
+        return -1;
+    }
+    if (hdr && hdrCap) {
+        const size_t n = std::min((size_t)hn, hdrCap - 1);
+        std::memcpy(hdr, h, n);
+        hdr[n] = 0;
+    }
+    // Prime::PrimeMapSize(): (maxPrimeMapValue + 15) >> 4 bytes; the device map covers
+    // (maxPrimeMapValue + 1 + 15) >> 4 bytes, at most one more
+    const uint64_t size = (g.mpv + 15) >> 4;
+    const uint64_t dev_bytes = (((g.mpv + 1 + 15) >> 4) + 255) & ~255ull;
+    uint8_t* d = nullptr;
+    uint8_t* out = (uint8_t*)std::malloc(size ? size : 1);
+    if (!out) return -1;
+    cudaStream_t st = nullptr;
+    int rc = 0;
+    if (cudaSetDevice(deviceIndex) != cudaSuccess || cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&d, dev_bytes) != cudaSuccess) {
+        rc = -1;
+    } else if (ffb_sieve_map_async(deviceIndex, g.mpv, d, st) != 0 ||
+               cudaMemcpyAsync(out, d, size, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+               cudaStreamSynchronize(st) != cudaSuccess) {
+        rc = -1;
+    }
+    if (d) cudaFree(d);
+    if (st) cudaStreamDestroy(st);
+    if (rc) {
+        std::fprintf(stderr, "ffb_map_dump: failed: %s\n", cudaGetErrorString(cudaGetLastError()));
+        std::free(out);
+        return -1;
+    }
+    *map = out;
+    *bytes = size;
+    return 0;
+}

@@ -134,6 +134,9 @@ SIGNATURES = {
     "ffb_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
                                ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]),
     "ffb_free": (None, [ctypes.c_void_p]),
+    "ffb_map_dump": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
+                                    ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_uint64),
+                                    ctypes.c_char_p, ctypes.c_size_t]),
     "ffb_emit": (ctypes.c_int, [ctypes.c_int, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p,
                                 ctypes.c_uint32, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
                                 ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]),
@@ -239,6 +242,22 @@ def emit(args, records, rec_lo, prime_us=0.0, freud_us=0.0):
         raise ValueError(f"ffb_emit{tuple(args)} failed")
     try:
         return ctypes.string_at(p, n.value)
+    finally:
+        lib.ffb_free(p)
+
+
+def map_dump(*args, dev=0):
+    """ffb_map_dump: (map bytes, header text) of `ff_seg --dump-map <file> <args>`."""
+    lib = load()
+    p = ctypes.c_void_p()
+    n = ctypes.c_uint64()
+    hdr = ctypes.create_string_buffer(4096)
+    a = [int(x) for x in args] + [0, 0]
+    if lib.ffb_map_dump(dev, len(args), a[0], a[1], ctypes.byref(p), ctypes.byref(n), hdr,
+                        len(hdr)) != 0:
+        raise RuntimeError(f"ffb_map_dump{args} failed")
+    try:
+        return ctypes.string_at(p, n.value), hdr.value
     finally:
         lib.ffb_free(p)
 

@@ -2,6 +2,11 @@
 // source/main.cpp:577-598 with ff_seg's positional semantics, reference/segmentedSieve.C:
 // 844-855). stdout carries exactly what ff_seg prints; stderr carries diagnostics.
 // Return code 0 on success, 1 on any error.
+//
+// `ff_sieve --dump-map <file> [<sumStart>] [<sumLimit>]` is ff_seg's sieve-only test option
+// (reference/segmentedSieve.C:830-839, 883-897): the header lines on stdout, the prime map
+// (Prime::PrimeMapSize() bytes) written to <file>, no search; its messages and exit codes
+// are ff_seg's (-6 no file argument or file not writable, -7 write failed).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -12,13 +17,49 @@ static void usage()
 {
     std::fprintf(stderr,
                  "usage: ff_sieve [--device N] [<sumStart>] [<sumLimit>]\n"
+                 "       ff_sieve --dump-map <file> [<sumStart>] [<sumLimit>]\n"
                  "  one positional argument: sums 5..<sumLimit>; none: 5..2627\n");
+}
+
+static int dump_map(int device, const char* file, int nargs, const int32_t* a)
+{
+    uint8_t* map = nullptr;
+    uint64_t bytes = 0;
+    char hdr[4096];
+    if (ffb_map_dump(device, nargs, a[0], a[1], &map, &bytes, hdr, sizeof hdr) != 0) return 1;
+    std::fputs(hdr, stdout);
+    std::fflush(stdout);
+    FILE* f = std::fopen(file, "wb");
+    if (!f) {
+        std::printf("Cannot open dump file '%s' for writing.\n", file);
+        ffb_free(map);
+        return -6;
+    }
+    const bool ok = std::fwrite(map, 1, bytes, f) == bytes;
+    ffb_free(map);
+    if (std::fclose(f) != 0 || !ok) {
+        std::printf("Failed to write dump file '%s'.\n", file);
+        return -7;
+    }
+    return 0;
 }
 
 int main(int argc, char** argv)
 {
     int device = 0, nargs = 0;
     int32_t a[2] = {0, 0};
+    if (argc > 1 && !std::strcmp(argv[1], "--dump-map")) {
+        if (argc < 3) {
+            std::printf("--dump-map requires a file argument.\n");
+            return -6;
+        }
+        const char* file = argv[2];
+        for (int i = 3; i < argc; ++i) {
+            if (!std::strcmp(argv[i], "--device") && i + 1 < argc) device = std::atoi(argv[++i]);
+            else if (nargs < 2) a[nargs++] = std::atoi(argv[i]);
+        }
+        return dump_map(device, file, nargs, a);
+    }
     for (int i = 1; i < argc; ++i) {
         if (!std::strcmp(argv[i], "--device") && i + 1 < argc) {
             device = std::atoi(argv[++i]);

@@ -380,6 +380,14 @@ void ffb_serve_destroy(FfbServer* s);
  * (a temporary context is used). */
 int ffb_run(FfbContext* ctx, int nargs, int32_t a1, int32_t a2, char** text, size_t* len);
 
+/* `ff_seg --dump-map <file> [<sumStart>] [<sumLimit>]` (reference/segmentedSieve.C:830-839,
+ * 883-897): the prime map of `ff_sieve <a1> <a2>` (see ffb_geometry), values up to its
+ * maxPrimeMapValue in the reference layout, Prime::PrimeMapSize() = (maxPrimeMapValue+15)>>4
+ * bytes, sieved on the device into a malloc'd host buffer (*map, free with ffb_free; *bytes
+ * its size). hdr (optional) receives the header lines ff_seg prints before it dumps. */
+int ffb_map_dump(int deviceIndex, int nargs, int32_t a1, int32_t a2, uint8_t** map,
+                 uint64_t* bytes, char* hdr, size_t hdrCap);
+
 /* The ff_sieve / ff_seg stdout for the given arguments from packed records already computed
  * (host memory, the format of ffb_search_async: h_rec[(s-recLo)/2] for odd sums
  * s = recLo, recLo+2, ..., covering every sum of the schedule), with the given timing

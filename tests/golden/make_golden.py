@@ -11,9 +11,12 @@ scripts/verify.sh does, and writes:
                          taken from the reference's goldens/SHA256SUMS and scripts/verify.sh
   small_ranges.json      stdout of ff_seg for short ranges, partition-quirk ranges
                          (fewer than 62 sums) and limits that take main's two-call split
+  dump_maps.json         with --dump-maps (only this file is written then): for argument
+                         lists of `ff_seg --dump-map <file> ...`, the size and sha256 of the
+                         dumped prime map and the stdout printed before the dump
 
 Needs the reference checkout; run from the repository root:
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py [--dump-maps]
 """
 import hashlib
 import json
@@ -90,5 +93,34 @@ def main():
     print(f"wrote {len(out)} small ranges, legs.json, out_ff_seg_65536.txt")
 
 
+def dump_maps():
+    """ff_seg --dump-map <file> <args> (reference/segmentedSieve.C:830-839, 883-897)."""
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    cases = [[], [100], [4, 17], [1000, 3000], [5, 65536], [5, 131072], [5, 262144],
+             [300001, 300100]]
+    out = []
+    for c in cases:
+        d = tempfile.mkdtemp()
+        dump = os.path.join(d, "map.bin")
+        try:
+            res = subprocess.run([REF_BIN, "--dump-map", dump] + [str(a) for a in c], cwd=d,
+                                 capture_output=True, check=True)
+            with open(dump, "rb") as f:
+                data = f.read()
+        finally:
+            if os.path.exists(dump):
+                os.remove(dump)
+            os.rmdir(d)
+        out.append({"args": c, "bytes": len(data), "sha256": hashlib.sha256(data).hexdigest(),
+                    "stdout": res.stdout.decode()})
+    with open(os.path.join(OUT, "dump_maps.json"), "w") as f:
+        json.dump(out, f, indent=1)
+    print(f"wrote {len(out)} map dumps to dump_maps.json")
+
+
 if __name__ == "__main__":
-    main()
+    import sys
+    if "--dump-maps" in sys.argv:
+        dump_maps()
+    else:
+        main()
