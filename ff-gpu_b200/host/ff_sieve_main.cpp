@@ -6,7 +6,9 @@
 // `ff_sieve --dump-map <file> [<sumStart>] [<sumLimit>]` is ff_seg's sieve-only test option
 // (reference/segmentedSieve.C:830-839, 883-897): the header lines on stdout, the prime map
 // (Prime::PrimeMapSize() bytes) written to <file>, no search; its messages and exit codes
-// are ff_seg's (-6 no file argument or file not writable, -7 write failed).
+// are ff_seg's (-6 no file argument or file not writable, -7 write failed). The flags that
+// the reference's scripts/verify.sh passes to its GPU binary (--devices nvidia, --gpu-search,
+// --dump-map <file> in any position) are accepted, so that harness runs unchanged.
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -16,8 +18,8 @@
 static void usage()
 {
     std::fprintf(stderr,
-                 "usage: ff_sieve [--device N] [<sumStart>] [<sumLimit>]\n"
-                 "       ff_sieve --dump-map <file> [<sumStart>] [<sumLimit>]\n"
+                 "usage: ff_sieve [--device N] [--devices nvidia] [--gpu-search]\n"
+                 "                [--dump-map <file>] [<sumStart>] [<sumLimit>]\n"
                  "  one positional argument: sums 5..<sumLimit>; none: 5..2627\n");
 }
 
@@ -60,9 +62,23 @@ int main(int argc, char** argv)
         }
         return dump_map(device, file, nargs, a);
     }
+    const char* dump = nullptr;
     for (int i = 1; i < argc; ++i) {
         if (!std::strcmp(argv[i], "--device") && i + 1 < argc) {
             device = std::atoi(argv[++i]);
+        } else if (!std::strcmp(argv[i], "--devices") && i + 1 < argc) {
+            // the reference's vendor filter (source/config.cpp:353-363): only CUDA devices here
+            const char* b = argv[++i];
+            if (std::strcmp(b, "nvidia") && std::strcmp(b, "NVIDIA")) {
+                std::fprintf(stderr, "ff_sieve: --devices %s: this build runs on NVIDIA "
+                             "(sm_100a) devices only\n", b);
+                return 1;
+            }
+        } else if (!std::strcmp(argv[i], "--gpu-search")) {
+            // the reference's switch to its GPU search (source/config.cpp:375-378): the
+            // search always runs on the GPU here
+        } else if (!std::strcmp(argv[i], "--dump-map") && i + 1 < argc) {
+            dump = argv[++i];  // ff_sieve's form (source/config.cpp:365-369): any position
         } else if (!std::strcmp(argv[i], "--help") || !std::strcmp(argv[i], "-h")) {
             usage();
             return 0;
@@ -77,6 +93,7 @@ int main(int argc, char** argv)
             return 1;
         }
     }
+    if (dump) return dump_map(device, dump, nargs, a);
     FfbContext* ctx = ffb_context_create(device);
     if (!ctx) {
         std::fprintf(stderr, "ff_sieve: no usable CUDA device %d\n", device);

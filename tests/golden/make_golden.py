@@ -11,12 +11,16 @@ scripts/verify.sh does, and writes:
                          taken from the reference's goldens/SHA256SUMS and scripts/verify.sh
   small_ranges.json      stdout of ff_seg for short ranges, partition-quirk ranges
                          (fewer than 62 sums) and limits that take main's two-call split
+  pen_blocks.json        with --pen-blocks (only this file is written then): per leg, the
+                         sha256 and line count of the solution block (the `) sum` lines) of
+                         the reference's goldens/out_pen_<leg>.txt and out_pen2_<leg>.txt,
+                         the second comparison of scripts/verify.sh:146-154
   dump_maps.json         with --dump-maps (only this file is written then): for argument
                          lists of `ff_seg --dump-map <file> ...`, the size and sha256 of the
                          dumped prime map and the stdout printed before the dump
 
 Needs the reference checkout; run from the repository root:
-    python tests/golden/make_golden.py [--dump-maps]
+    python tests/golden/make_golden.py [--dump-maps | --pen-blocks]
 """
 import hashlib
 import json
@@ -118,9 +122,27 @@ def dump_maps():
     print(f"wrote {len(out)} map dumps to dump_maps.json")
 
 
+def pen_blocks():
+    """Solution blocks of the pen/pen2 goldens (scripts/verify.sh:146-154: grep ') sum')."""
+    out = {}
+    for leg in (65536, 131072, 262144, 524288, 1048576):
+        row = {}
+        for kind in ("pen", "pen2", "ff_seg"):
+            with open(os.path.join(REF_TREE, "goldens", f"out_{kind}_{leg}.txt"), "rb") as f:
+                lines = [ln for ln in f.read().split(b"\n") if b") sum" in ln]
+            block = b"".join(ln + b"\n" for ln in lines)
+            row[kind] = {"sha256": hashlib.sha256(block).hexdigest(), "lines": len(lines)}
+        out[str(leg)] = row
+    with open(os.path.join(OUT, "pen_blocks.json"), "w") as f:
+        json.dump(out, f, indent=1, sort_keys=True)
+    print(f"wrote pen_blocks.json for {len(out)} legs")
+
+
 if __name__ == "__main__":
     import sys
     if "--dump-maps" in sys.argv:
         dump_maps()
+    elif "--pen-blocks" in sys.argv:
+        pen_blocks()
     else:
         main()
