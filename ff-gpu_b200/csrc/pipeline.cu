@@ -27,6 +27,7 @@ struct FfbContext {
     uint64_t rec_cap = 0;
     uint64_t* h_rec = nullptr;  // pinned
     uint64_t hrec_cap = 0;
+    uint64_t map_budget = 0;    // cap on the map's bytes (0: the device's free memory)
 };
 
 namespace ffb {
@@ -57,6 +58,30 @@ int grow(FfbContext* c, uint64_t map_bytes, uint64_t nrec)
         c->hrec_cap = nrec;
     }
     return 0;
+}
+
+// The map bound of a job: `want` (every value the job may probe) when that map fits the
+// device-memory budget (the reference's computeBudget on the free memory, source/budget.cpp:
+// 15-42, less the job's records), else the largest map that fits; the search answers the
+// probes above it by Miller-Rabin, which is exact, so the output is the same either way
+// (the reference likewise caps its own map, reference/segmentedSieve.C:148-176). 0: no room.
+uint64_t fit_map_mpv(FfbContext* c, uint64_t want, uint64_t nrec)
+{
+    size_t free_b = 0, total_b = 0;
+    if (cudaSetDevice(c->dev) != cudaSuccess || cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        free_b = 0;
+    }
+    // the context's own buffers are freed and made again when they must grow
+    const uint64_t own = c->map_cap + 8 * c->rec_cap;
+    FfbBudget b{};
+    ffb_compute_budget(free_b + own, 0.90, 0, 0, 0, &b);
+    uint64_t avail = b.backing > 16 * nrec ? b.backing - 16 * nrec : 0;
+    if (c->map_budget && c->map_budget < avail) avail = c->map_budget;
+    const uint64_t want_bytes = (want + 1 + 15) >> 4;
+    if (want_bytes + 256 <= avail) return want;
+    const uint64_t bytes = (avail > 256 ? avail - 256 : 0) & ~255ull;
+    return bytes >= 4096 ? bytes * 16 - 1 : 0;
 }
 
 // Text of the solution lines of the schedule, numbered from 1 in emission order.
@@ -138,6 +163,13 @@ extern "C" void ffb_context_destroy(FfbContext* c)
     delete c;
 }
 
+extern "C" int ffb_context_set_map_budget(FfbContext* ctx, uint64_t bytes)
+{
+    if (!ctx) return -1;
+    ctx->map_budget = bytes;
+    return 0;
+}
+
 extern "C" void ffb_free(void* p) { std::free(p); }
 
 extern "C" int ffb_run(FfbContext* ctx, int nargs, int32_t a1, int32_t a2, char** text, size_t* len)
@@ -172,18 +204,25 @@ extern "C" int ffb_run(FfbContext* ctx, int nargs, int32_t a1, int32_t a2, char*
         return -1;
     }
     // The device map: the reference's (values up to mpv) or, when larger, one covering every
-    // value the search probes, so that no probe falls back to Miller-Rabin. IsPrime is exact
-    // either way, so the output does not depend on this choice.
-    uint64_t map_mpv = g.mpv;
-    if (lo <= hi) map_mpv = std::max(map_mpv, ffb_probe_bound(hi));
-    const uint64_t map_bytes = (map_mpv + 1 + 15) >> 4;
+    // value the search probes, so that no probe falls back to Miller-Rabin, as far as device
+    // memory allows (fit_map_mpv). IsPrime is exact either way, so the output does not
+    // depend on this choice.
+    uint64_t want = g.mpv;
+    if (lo <= hi) want = std::max(want, ffb_probe_bound(hi));
     FfbContext* c = ctx ? ctx : ffb_context_create(0);
     if (!c) return -1;
+    const uint64_t nrec = lo <= hi ? ((uint64_t)hi - lo) / 2 + 1 : 1;
+    const uint64_t map_mpv = fit_map_mpv(c, want, nrec);
+    const uint64_t map_bytes = (map_mpv + 1 + 15) >> 4;
     int rc = 0;
     std::string body;
     double prime_us = 0, freud_us = 0;
     do {
-        const uint64_t nrec = lo <= hi ? ((uint64_t)hi - lo) / 2 + 1 : 1;
+        if (!map_mpv) {
+            std::fprintf(stderr, "ffb_run: no device memory left for a prime map\n");
+            rc = -1;
+            break;
+        }
         if ((rc = grow(c, map_bytes, nrec))) break;
         cudaSetDevice(c->dev);
         const auto t0 = clk::now();

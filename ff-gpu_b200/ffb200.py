@@ -131,6 +131,7 @@ SIGNATURES = {
                                           ctypes.c_void_p, ctypes.c_void_p]),
     "ffb_context_create": (ctypes.c_void_p, [ctypes.c_int]),
     "ffb_context_destroy": (None, [ctypes.c_void_p]),
+    "ffb_context_set_map_budget": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64]),
     "ffb_run": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int32, ctypes.c_int32,
                                ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(ctypes.c_size_t)]),
     "ffb_free": (None, [ctypes.c_void_p]),

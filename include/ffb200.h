@@ -247,6 +247,13 @@ int ffb_take_errors(int deviceIndex, uint32_t* flags);
 typedef struct FfbContext FfbContext;
 FfbContext* ffb_context_create(int deviceIndex);
 void ffb_context_destroy(FfbContext* ctx);
+/* Caps the bytes of the context's prime map (0, the default: 90 % of the device's free
+ * memory less the job's records and the budget's scratch and headroom, as the reference's
+ * computeBudget, source/budget.cpp:15-42). A job whose probes need a larger map gets the
+ * largest map under the cap, and Miller-Rabin answers above it: the same output, more
+ * search time. The reference caps its own map the same way (PRIMEMEM,
+ * reference/segmentedSieve.C:148-176). */
+int ffb_context_set_map_budget(FfbContext* ctx, uint64_t bytes);
 
 /* A batch of ff_sieve runs (no reference counterpart): n ranges, each given as the two
  * atoi()-style arguments of `ff_sieve <sumStart> <sumLimit>`, evaluated together. One prime

@@ -114,3 +114,20 @@ def test_output_independent_of_map_bound_on_gpu(ffb, oracle):
     assert torch.equal(a, b)
     assert int((a != 0).sum()) > 0
     assert ffb.take_errors() == 0
+
+
+@pytest.mark.parametrize("args,budget", [((5, 262144), 64 << 20), ((5, 65536), 1 << 20)])
+def test_run_with_a_capped_map(ffb, golden, args, budget):
+    """ffb_run under a map budget far below the job's map (the path a job whose map exceeds
+    device memory takes): the largest map under the cap, Miller-Rabin above it, and the
+    text still ff_seg's."""
+    lib = ffb.load()
+    ctx = lib.ffb_context_create(0)
+    try:
+        assert lib.ffb_context_set_map_budget(ctx, budget) == 0
+        text = ffb.run(*args, ctx=ctx)
+    finally:
+        lib.ffb_context_destroy(ctx)
+    leg = golden["legs"][str(args[1])]
+    assert hashlib.sha256(norm(text)).hexdigest() == leg["sha256"]
+    assert ffb.take_errors() == 0
