@@ -33,7 +33,7 @@ struct SearchArgs {
                             // chunk}, largest sums first (or null: the single range lo..hi)
     uint32_t nseg = 0;      // intervals in seg (0: single range)
     uint32_t nchunks = 0;   // chunks of 32 sums over all intervals
-    uint32_t warps = 0;     // warps per block: 4, 8 or 16 (0: 8)
+    uint32_t warps = 0;     // warps per block: 4, 8 or 16 (0: 16 map-only, 8 Miller-Rabin)
 };
 
 // Packed per-sum record written by the search: 0 = no solution line, else
