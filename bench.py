@@ -229,18 +229,29 @@ def ours(args, rank, world, dist):
                 "algorithmic_bytes": alg, "stage1_probes": probes_per_step,
                 "stage2_items": stage2_per_step, "peak_source": peak_src,
                 "note": "latency-bound integer kernel; see profiles/ for pipe utilisation"}
+    def optional(fn, *a):
+        # a side section that fails (e.g. a box with less free memory) is reported in its
+        # place; the measured line above it is printed either way
+        try:
+            return fn(*a)
+        except Exception as e:  # noqa: BLE001
+            print(f"bench.py: {fn.__name__} failed: {e!r}", file=sys.stderr, flush=True)
+            return {"error": repr(e)[:300]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args)
+        cpu = optional(cpu_baseline, args)
     batched = None
     if rank == 0 and world == 1 and not args.no_batched and LIMIT == 2097152:
-        batched = batched_section(args, dev)
+        batched = optional(batched_section, args, dev)
     served = None
     if rank == 0 and world == 1 and args.served_requests > 0 and LIMIT == 2097152:
-        served = served_section(args, dev)
+        del d_map
+        torch.cuda.empty_cache()
+        served = optional(served_section, args, dev)
     sweep = None
     if rank == 0 and world == 1 and not args.no_sieve_sweep and LIMIT == 2097152:
-        sweep = sieve_sweep_section(args, dev, hbm_peak)
+        sweep = optional(sieve_sweep_section, args, dev, hbm_peak)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
