@@ -7,22 +7,30 @@ over the odd sums 5..2^21 (`ff_sieve 5 2097152`), byte-identical to the referenc
 One step = the whole job for the range: the prime map sieved on the device (the reference's
 16 GiB map for values up to 274,877,906,959, extended to the 21.3 GiB that every probe of
 the search needs so that none falls back to Miller-Rabin), then every odd sum of the range
-searched, leaving one packed record per sum in HBM. `value` is odd sums per second of that job on
-device-resident data (CUDA events on the launching stream, max over ranks); `e2e` is the
-same metric through the public call a user makes (ffb_run: sieve, search, records copied
-to the host, the text emitted in ff_seg's order), timed on the host clock.
+searched, leaving one packed record per sum in HBM. `value` is odd sums per second of that
+job on device-resident data (CUDA events on the launching stream, max over ranks); `e2e` is
+the same metric through the public call a user makes (ffb_run: sieve, search, records copied
+to the host, the text emitted in ff_seg's order), timed on the host clock. After the timed
+steps the records are emitted as text and checked against the reference's SHA-256 of the
+2^21 leg; a mismatch fails the run.
 
 --impl reference times the reference program itself (ff_seg, compiled from the
 reference's source) on the host cores: a bounded sample of the same job (see
 reference_arm()).
 
-With N > 1 ranks (torchrun), the sums are split into cost-balanced contiguous shards, one
-per GPU; each rank sieves the map its shard needs and searches its shard, and the records
-are gathered to rank 0 over NCCL (strong scaling: the job is fixed).
+With N > 1 ranks (torchrun), each rank sieves an equal slab of the map and an NCCL
+all-gather assembles the whole map on every rank; the sums are split into cost-balanced
+contiguous shards, one per GPU, searched with no exchange, and the records are gathered to
+rank 0 (strong scaling: the job is fixed).
+
+The side sections (batched, served, sieve sweep) run on rank 0 of a 1-GPU run; a compact
+summary of every section is the last key of the JSON line.
 """
 import argparse
 import ctypes
+import hashlib
 import json
+import math
 import os
 import re
 import statistics
@@ -38,10 +46,36 @@ sys.path.insert(0, os.path.join(ROOT, "ff-gpu_b200"))
 LIMIT = 2097152
 METRIC = "sums/sec byte-identical at sumLimit=2^21; served p50/p99 latency vs plain"
 UNIT = "sums/s"
+NORM = re.compile(rb"(Prime|Freudenthal) time: [0-9]+")
+DEFAULT_TILE = 96 * 1024    # the sieve's shared-memory tile when the caller does not choose
+
+# Integer operations per occurrence of each primitive of the reference search, counted as
+# the 32-bit integer instructions (IMAD or ALU) an implementation needs:
+#   isprime_calls  IsPrime from the map: parity test, bound compare, byte index, load, bit
+#                  shift, mask                                                          6
+#   splits         one (evenTerm, oddTerm) decomposition: b = s - o*2^k, o mod 3 and b mod 3
+#                  (multiply-high), the 64-bit pair sums and the branch                 12
+#   abop_calls     AllButOne... set-up: the 64-bit product, isqrt64, the first pair     18
+#   trial_steps    one trial division of the product: a 64-bit by 32-bit quotient by
+#                  reciprocal multiply and the exactness test                           10
+#   divisors       one divisor pair: the 64-bit multiple, the 64-bit quotient product/d,
+#                  the pair sum, the bound test and the list append                     18
+# The counts per job come from the instrumented CPU restatement of the reference
+# (tests/golden/search_work.json, made by tests/golden/make_search_work.py).
+OP_COST = {"isprime_calls": 6, "splits": 12, "abop_calls": 18, "trial_steps": 10, "divisors": 18}
 
 
 def odd_sums(lo, hi):
     return (hi - lo) // 2 + 1 if hi >= lo else 0
+
+
+def norm(b):
+    return NORM.sub(rb"\1 time: N", b)
+
+
+def golden(name):
+    with open(os.path.join(ROOT, "tests", "golden", name)) as f:
+        return json.load(f)
 
 
 # ---------------------------------------------------------------------------------------
@@ -99,45 +133,109 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------------------
+# roofline helpers
+# ---------------------------------------------------------------------------------------
+def hbm_peak():
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    if "hbm_gbs" in peaks:
+        return float(peaks["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return 6650.0, "fallback (6.65 TB/s, an earlier measurement on this pool)"
+
+
+def odd_primes_upto(n):
+    import numpy as np
+    if n < 3:
+        return np.zeros(0, dtype=np.int64)
+    s = np.ones((n - 1) // 2, dtype=bool)   # index j -> 2j+3
+    for j in range(int((math.isqrt(n) - 1) // 2)):
+        if s[j]:
+            p = 2 * j + 3
+            s[(p * p - 3) // 2::p] = False
+    return 2 * np.nonzero(s)[0].astype(np.int64) + 3
+
+
+def sieve_marks(mpv, tile_bytes):
+    """Shared-memory marks sieve_tiles makes for the map of values 0..mpv: the comb primes
+    (41 <= p <= tile bits / 1024) mark every odd multiple from p^2, the larger primes the
+    multiples p*k, k >= p, with k prime to 30 (the patterns cover 3..37)."""
+    import numpy as np
+    p = odd_primes_upto(math.isqrt(mpv))
+    p = p[p >= 41]
+    pcomb = tile_bytes * 8 // 1024
+    comb = p[p <= pcomb]
+    wheel = p[p > pcomb]
+    n_comb = int(((mpv - comb * comb) // (2 * comb) + 1).sum())
+
+    def coprime30_upto(x):   # #{1 <= k <= x : gcd(k, 30) = 1}
+        r = x % 30
+        small = np.zeros_like(x)
+        for res in (1, 7, 11, 13, 17, 19, 23, 29):
+            small += (r >= res)
+        return 8 * (x // 30) + small
+    kmax = mpv // wheel
+    n_wheel = int((coprime30_upto(kmax) - coprime30_upto(wheel - 1)).sum())
+    return n_comb, n_wheel
+
+
+def search_ops():
+    w = golden("search_work.json")["per_job"]
+    return sum(w[k] * c for k, c in OP_COST.items()), w
+
+
+# ---------------------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------------------
-def geometry_for(ffb, limit):
-    g, _ = ffb.geometry(5, limit)
-    return g
-
-
 def ours(args, rank, world, dist):
     import torch
     import ffb200 as ffb
-    from shard import shard_bounds, gather_records
+    from shard import gather_map, gather_records, map_slab, shard_bounds
     lib = ffb.load()
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
-    g = geometry_for(ffb, LIMIT)
+    peaks = ffb.measure_peaks(dev)
+    g, _ = ffb.geometry(5, LIMIT)
     lo, hi = 5, LIMIT - 1                                  # odd sums of `ff_sieve 5 2097152`
     a, b = shard_bounds(lo, hi, world, rank)
-    # the map this shard's probes need: the reference's map for the shard's top sum, or the
-    # larger bound under which every probe of the search is a map lookup (ffb_probe_bound;
-    # the output is the same either way, Miller-Rabin being exact)
-    gs = geometry_for(ffb, b + 1)
-    mpv = max(gs.maxPrimeMapValue, lib.ffb_probe_bound(b))
+    # the map: the reference's map, or the larger bound under which every probe of the
+    # search is a map lookup (ffb_probe_bound; the output is the same either way,
+    # Miller-Rabin being exact)
+    mpv = max(g.maxPrimeMapValue, lib.ffb_probe_bound(hi))
     if args.map_bound:          # a smaller map: probes above it go to the Miller-Rabin variant
         mpv = min(mpv, (args.map_bound + 1) // 16 * 16 - 1)
+    map_bytes = (mpv + 1 + 15) >> 4
+    if world > 1:
+        seg_lo, seg_hi, slab = map_slab(mpv, world, rank)
+        d_map = torch.empty(world * slab + 256, dtype=torch.uint8, device="cuda")
+    else:
+        seg_lo, seg_hi, slab = 0, mpv + 1, 0
+        d_map = torch.empty(map_bytes + 256, dtype=torch.uint8, device="cuda")
     nsums = odd_sums(a, b)
-    d_map = torch.empty(((mpv + 1 + 15) >> 4) + 64, dtype=torch.uint8, device="cuda")
     d_rec = torch.empty(max(nsums, 1), dtype=torch.int64, device="cuda")
     stream = torch.cuda.Stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
 
     def step(ev=None):
-        if ev:
-            ev[0].record(stream)
-        assert lib.ffb_sieve_map_async(dev, mpv, d_map.data_ptr(), sp) == 0
-        if ev:
-            ev[1].record(stream)
-        assert lib.ffb_search_async(dev, d_map.data_ptr(), mpv, a, b, d_rec.data_ptr(), sp) == 0
-        if ev:
-            ev[2].record(stream)
+        with torch.cuda.stream(stream):
+            if ev:
+                ev[0].record(stream)
+            if world > 1:
+                if seg_hi > seg_lo:
+                    assert lib.ffb_sieve_map_range_async(dev, seg_lo, seg_hi,
+                                                         d_map.data_ptr() + (seg_lo >> 4), sp) == 0
+                gather_map(dist, d_map, slab)
+            else:
+                assert lib.ffb_sieve_map_async(dev, mpv, d_map.data_ptr(), sp) == 0
+            if ev:
+                ev[1].record(stream)
+            if a <= b:
+                assert lib.ffb_search_async(dev, d_map.data_ptr(), mpv, a, b, d_rec.data_ptr(), sp) == 0
+            if ev:
+                ev[2].record(stream)
 
     for _ in range(args.warmup):
         step()
@@ -170,9 +268,22 @@ def ours(args, rank, world, dist):
     lib.ffb_search_stats(dev, stats, 1)
     probes_per_step = stats[0] // args.steps
     stage2_per_step = stats[1] // args.steps
-    # records of all shards to rank 0 (the exchange of the sharded job)
+    # the records of all shards on rank 0, emitted as ff_seg's text and checked against the
+    # reference's hash of the leg (outside the timed region; a mismatch fails the run)
     if dist and world > 1:
-        gather_records(dist, d_rec, lo, hi, world, rank)
+        full = gather_records(dist, d_rec, lo, hi, world, rank)
+    else:
+        full = d_rec
+    verified = None
+    if rank == 0:
+        import numpy as np
+        text = ffb.emit((5, LIMIT), full.cpu().numpy().view(np.uint64), lo)
+        want = golden("legs.json")[str(LIMIT)]["sha256"] if LIMIT == 2097152 else None
+        got = hashlib.sha256(norm(text)).hexdigest()
+        if want is not None and got != want:
+            raise RuntimeError(f"the job's text differs from the reference leg: sha256 {got}")
+        verified = {"sha256": got, "equals_reference_leg": want is not None,
+                    "solutions": text.count(b") sum =")}
     t = torch.tensor([total_ms, sieve_ms, search_ms], dtype=torch.float64, device="cuda")
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -202,33 +313,41 @@ def ours(args, rank, world, dist):
                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8 * job_sums,
                "text_bytes_per_step": text_len, "ms_per_step": 1e3 * statistics.mean(times)}
 
-    peaks = {}
-    try:
-        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
-            peaks = json.load(f)
-    except OSError:
-        pass
-    hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    map_bytes = (mpv + 1 + 15) >> 4
-    # dominant kernel of the step
-    if sieve_ms >= search_ms:
-        achieved = map_bytes / (sieve_ms / 1e3) / 1e9
-        roof = {"kernel": "sieve_tiles", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
-                "algorithmic_bytes": map_bytes, "peak_source": peak_src,
-                "note": "algorithmic bytes = bitmap bytes written once"}
-    else:
-        # search: each stage-1 probe (2^k + o*b - 2) reads one random 32-byte sector of the
-        # multi-GB map; the records are written once. Algorithmic bytes per step =
-        # 32 B x stage-1 probes + 8 B x sums (counted on the device in the timed steps).
-        alg = 32 * probes_per_step + 8 * nsums
-        achieved = alg / (search_ms / 1e3) / 1e9
-        roof = {"kernel": "search_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm_peak,
-                "unit": "GB/s", "frac": achieved / hbm_peak, "traffic": None,
-                "algorithmic_bytes": alg, "stage1_probes": probes_per_step,
-                "stage2_items": stage2_per_step, "peak_source": peak_src,
-                "note": "latency-bound integer kernel; see profiles/ for pipe utilisation"}
+    hbm, hbm_src = hbm_peak()
+    # sieve: HBM bytes written once, and the shared-memory marks against the measured atomic
+    # throughput (comb marks conflict-free, one-thread-per-prime marks on random banks)
+    sieve_bytes = (seg_hi - seg_lo + 15) >> 4 if world > 1 else map_bytes
+    n_comb, n_wheel = sieve_marks(mpv, DEFAULT_TILE)
+    if world > 1:
+        n_comb, n_wheel = n_comb / world, n_wheel / world
+    mark_floor_s = n_comb / peaks["atomsConflictFreePerS"] + n_wheel / peaks["atomsRandomPerS"]
+    sieve_kernel_s = sieve_ms / 1e3
+    sieve_roof = {
+        "kernel": "sieve_tiles", "bound": "hbm", "achieved": sieve_bytes / sieve_kernel_s / 1e9,
+        "peak": hbm, "unit": "GB/s", "frac": sieve_bytes / sieve_kernel_s / 1e9 / hbm,
+        "traffic": None, "peak_source": hbm_src, "algorithmic_bytes": sieve_bytes,
+        "marks": n_comb + n_wheel, "marks_per_s": (n_comb + n_wheel) / sieve_kernel_s,
+        "marking_floor_ms": 1e3 * mark_floor_s,
+        "frac_of_marking_floor": mark_floor_s / sieve_kernel_s,
+        "note": "algorithmic bytes = bitmap bytes written once; marking floor = marks at the "
+                "measured shared-memory atomicAnd rates (ffb_measure_peaks)"
+                + ("; sieve_ms includes the NCCL all-gather of the map" if world > 1 else "")}
+    ops, work = search_ops()
+    if world > 1:
+        share = (b * b - a * a) / (hi * hi - lo * lo) if a <= b else 0.0
+        ops *= share
+    search_roof = {
+        "kernel": "search_kernel", "bound": "int_alu", "achieved": ops / (search_ms / 1e3),
+        "peak": peaks["intOpsPerS"], "unit": "int ops/s",
+        "frac": ops / (search_ms / 1e3) / peaks["intOpsPerS"], "traffic": None,
+        "peak_source": "measured (ffb_measure_peaks: integer multiply-add and ALU chains, "
+                       "one IMAD to two ALU operations, whole GPU)",
+        "algorithmic_ops": ops, "op_cost": OP_COST, "work_per_job": work,
+        "stage1_probes": probes_per_step, "stage2_items": stage2_per_step,
+        "note": "algorithmic ops = the reference search's primitive counts (instrumented CPU "
+                "restatement) x the op_cost table; the kernel is bound by map-probe latency"}
+    roof, other = (search_roof, sieve_roof) if search_ms >= sieve_ms else (sieve_roof, search_roof)
+
     def optional(fn, *a):
         # a side section that fails (e.g. a box with less free memory) is reported in its
         # place; the measured line above it is printed either way
@@ -238,20 +357,21 @@ def ours(args, rank, world, dist):
             print(f"bench.py: {fn.__name__} failed: {e!r}", file=sys.stderr, flush=True)
             return {"error": repr(e)[:300]}
 
+    side = rank == 0 and world == 1 and LIMIT == 2097152
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = optional(cpu_baseline, args)
     batched = None
-    if rank == 0 and world == 1 and not args.no_batched and LIMIT == 2097152:
+    if side and not args.no_batched:
         batched = optional(batched_section, args, dev)
     served = None
-    if rank == 0 and world == 1 and args.served_requests > 0 and LIMIT == 2097152:
+    if side and args.served_requests > 0:
         del d_map
         torch.cuda.empty_cache()
         served = optional(served_section, args, dev)
     sweep = None
-    if rank == 0 and world == 1 and not args.no_sieve_sweep and LIMIT == 2097152:
-        sweep = optional(sieve_sweep_section, args, dev, hbm_peak)
+    if side and not args.no_sieve_sweep:
+        sweep = optional(sieve_sweep_section, args, dev, hbm, peaks)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -262,13 +382,104 @@ def ours(args, rank, world, dist):
                                    f"{g.maxPrimeMapValue}) + search of {job_sums} odd sums",
                        "sum_start": 5, "sum_limit": LIMIT, "map_bytes": map_bytes,
                        "l2": "inputs larger than L2 (the map is rewritten every step)",
-                       "parallelism": f"sum shards x{world}" if world > 1 else "1 GPU"},
+                       "parallelism": (f"map slabs + NCCL all-gather, sum shards x{world}"
+                                       if world > 1 else "1 GPU")},
             "kernel_ms": {"sieve_tiles": sieve_ms, "search_kernel": search_ms},
-            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "batched": batched, "served": served, "sieve_sweep": sweep,
-            "gpu_launches": 2 * args.steps,
+            "roofline": roof, "roofline_other": other, "peaks": peaks, "verified": verified,
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "sieve_sweep": sweep, "batched": batched, "served": served,
+            "gpu_launches": 3 * args.steps,   # list_primes, sieve_tiles, search_kernel per step
         }
+        line["summary"] = summary(line)
         print(json.dumps(line), flush=True)
+
+
+def summary(line):
+    """The numbers of every section in a few keys (printed last in the line)."""
+    def g(d, *ks):
+        for k in ks:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+    s = {"value": line["value"], "e2e": g(line, "e2e", "value"),
+         "sieve_ms": g(line, "kernel_ms", "sieve_tiles"),
+         "search_ms": g(line, "kernel_ms", "search_kernel"),
+         "roofline_frac": g(line, "roofline", "frac"),
+         "cpu_reference": g(line, "cpu_baseline", "value"),
+         "cpu_reference_nproc_threads": g(line, "cpu_baseline", "threads_nproc_minus_1", "value")}
+    b = line.get("batched") or {}
+    if "value" in b:
+        s["batched"] = {"requested_sums_per_s": b["value"],
+                        "distinct_sums_per_s": b.get("distinct_sums_per_s"),
+                        "vs_plain": b.get("vs_plain"), "cpu_sums_per_s": g(b, "cpu_baseline", "value")}
+    v = line.get("served") or {}
+    if "saturation" in v:
+        sat = v["saturation"]
+        s["served"] = {"requests": sat["requests"], "sums_per_s": sat["value"],
+                       "vs_plain": v.get("vs_plain"), "p50_ms": sat["latency_ms"]["p50"],
+                       "p99_ms": sat["latency_ms"]["p99"], "p999_ms": sat["latency_ms"]["p999"],
+                       "loads": [{"load": r["load"], "p50_ms": r["latency_ms"]["p50"],
+                                  "p99_ms": r["latency_ms"]["p99"], "p999_ms": r["latency_ms"]["p999"]}
+                                 for r in v.get("rates", [])],
+                       "cpu_sums_per_s": g(v, "cpu_baseline", "value")}
+    w = line.get("sieve_sweep") or {}
+    if "rows" in w:
+        s["sieve_sweep"] = {r["N"]: {"tile": r["best"]["tile"], "GB/s": r["best"]["GB/s"],
+                                     "cpu_GB/s": g(r, "cpu", "GB/s")} for r in w["rows"]}
+    return s
+
+
+# ---------------------------------------------------------------------------------------
+# CPU baselines of the side configurations: the restatement oracle, multithreaded on the
+# host's cores, on a bounded sample (test infrastructure used only as the CPU comparator)
+# ---------------------------------------------------------------------------------------
+def oracle_union_rate(arg_lists, windows=48, width=256):
+    """Odd sums per second of the CPU restatement searching the union of the ranges' sums
+    (each shared sum once, as the GPU batch does) with all host cores; measured on `windows`
+    windows of `width` consecutive odd sums spread over the union by position and scaled.
+    The map covers values up to 2^34 (Miller-Rabin above, exact); its sieve is not timed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ffo
+    spans = []
+    for a, b in arg_lists:
+        gg, _ = ffo.geometry(*ffo.parse_args(a, b))
+        for f, l in ffo.schedule(gg.sum_start, gg.sum_limit, gg.max_prime_map_value):
+            f |= 1
+            l -= 1 - (l & 1)
+            if f <= l:
+                spans.append((f, l))
+    spans.sort()
+    union = []
+    for f, l in spans:
+        if union and f <= union[-1][1] + 2:
+            union[-1][1] = max(union[-1][1], l)
+        else:
+            union.append([f, l])
+    total = sum(odd_sums(f, l) for f, l in union)
+    # window start positions: evenly spaced ordinals of the union's sums
+    cum, acc = [], 0
+    for f, l in union:
+        cum.append(acc)
+        acc += odd_sums(f, l)
+    threads = os.cpu_count() or 1
+    sampled, secs = 0, 0.0
+    top = max(l for _, l in union)
+    with ffo.Context(top + 2, map_bound=(1 << 34) - 1, threads=threads) as c:
+        for i in range(windows):
+            pos = (2 * i + 1) * total // (2 * windows)
+            j = max(k for k in range(len(union)) if cum[k] <= pos)
+            f, l = union[j]
+            s0 = f + 2 * (pos - cum[j])
+            s1 = min(l, s0 + 2 * (width - 1))
+            t = time.perf_counter()
+            c.eval_range(s0, s1, threads=threads)
+            secs += time.perf_counter() - t
+            sampled += odd_sums(s0, s1)
+    return {"value": sampled / secs, "unit": "distinct sums/s", "cores": threads, "kind": "port",
+            "union_sums": total, "est_union_s": total * secs / sampled,
+            "sample": f"{windows} windows of {width} odd sums over the union of the ranges' sums "
+                      f"({sampled} sums), oracle map to 2^34 + Miller-Rabin above, sieve untimed"}
 
 
 # ---------------------------------------------------------------------------------------
@@ -294,13 +505,15 @@ def batched_section(args, dev):
         times, dev_ms = [], []
         for _ in range(args.steps):
             s = time.perf_counter()
-            batch.run()
+            texts = batch.run()
             times.append(time.perf_counter() - s)
             info = batch.info()
             dev_ms.append(info["sieveMs"] + info["searchMs"])
         info = batch.info()
     finally:
         batch.close()
+    fix = golden("batched_seed0.json")["ranges"]
+    mismatches = sum(1 for r, t in zip(fix, texts) if hashlib.sha256(norm(t)).hexdigest() != r["sha256"])
     # the plain method, one ffb_run per range, on an evenly spaced sample of the ranges
     ctx = lib.ffb_context_create(dev)
     sample = ranges[::16]
@@ -317,34 +530,43 @@ def batched_section(args, dev):
             plain_sums += range_sums(a, b)
     finally:
         lib.ffb_context_destroy(ctx)
-    value = sums / statistics.mean(times)
+    t_batch = statistics.mean(times)
+    value = sums / t_batch
     plain = plain_sums / plain_t
-    return {"workload": "256 ranges from seed 0 (start U{5..2^21}, length floor(2^U[8,18]))",
-            "value": value, "unit": UNIT, "ms_per_batch": 1e3 * statistics.mean(times),
-            "device_ms_per_batch": statistics.mean(dev_ms), "sums_per_batch": sums,
-            "distinct_sums": info["sums"], "intervals": info["intervals"],
-            "map_bytes": info["mapBytes"], "sieve_tile_bytes": info["sieveTileBytes"],
-            "search_warps": info["searchWarps"], "setup_s_incl_autotune": setup_s,
-            "plain_one_launch_per_range": {"value": plain, "unit": UNIT,
-                                           "sample": f"{len(sample)} of the 256 ranges (every 16th)"},
-            "vs_plain": value / plain}
+    cpu = None if args.no_cpu_baseline else oracle_union_rate(ranges)
+    out = {"workload": "256 ranges from seed 0 (start U{5..2^21}, length floor(2^U[8,18]))",
+           "value": value, "unit": "requested sums/s", "ms_per_batch": 1e3 * t_batch,
+           "device_ms_per_batch": statistics.mean(dev_ms), "sums_per_batch": sums,
+           "distinct_sums": info["sums"], "distinct_sums_per_s": info["sums"] / t_batch,
+           "intervals": info["intervals"], "map_bytes": info["mapBytes"],
+           "tuned": {k: info[k] for k in ("sieveTileBytes", "searchWarps", "searchChunk",
+                                            "searchGroup") if k in info},
+           "setup_s_incl_autotune": setup_s, "oracle_mismatches": mismatches,
+           "plain_one_launch_per_range": {"value": plain, "unit": UNIT,
+                                          "sample": f"{len(sample)} of the 256 ranges (every 16th)"},
+           "vs_plain": value / plain}
+    if cpu:
+        cpu["est_batch_s"] = cpu["est_union_s"]
+        cpu["value_requested"] = sums / cpu["est_union_s"]
+        out["cpu_baseline"] = {**cpu, "value": cpu["value_requested"], "unit": "requested sums/s"}
+        out["vs_cpu"] = value / cpu["value_requested"]
+    return out
 
 
 # ---------------------------------------------------------------------------------------
 # sieve sweep: the map for N = 2^24, 2^28, 2^32 with the shared-memory tile swept
 # ---------------------------------------------------------------------------------------
-def sieve_sweep_section(args, dev, hbm_peak):
+def sieve_sweep_section(args, dev, hbm, peaks):
     import torch
     import ffb200 as ffb
     lib = ffb.load()
     stream = torch.cuda.Stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
-    marks = {24: 1.53e7, 28: 2.66e8, 32: 4.55e9}   # odd multiples >= p^2 of odd primes <= sqrt(N)
     out = []
     for logn in (24, 28, 32):
         n = 1 << logn
         nbytes = (n + 1 + 15) >> 4
-        d = torch.empty(nbytes + 64, dtype=torch.uint8, device="cuda")
+        d = torch.empty(nbytes + 256, dtype=torch.uint8, device="cuda")
         row = {"N": f"2^{logn}", "map_bytes": nbytes, "tiles": {}}
         for kb in (64, 96, 128, 160, 192, 216):
             for _ in range(3):
@@ -359,15 +581,33 @@ def sieve_sweep_section(args, dev, hbm_peak):
             e1.synchronize()
             ms = e0.elapsed_time(e1) / reps
             gbs = nbytes / (ms / 1e3) / 1e9
-            row["tiles"][f"{kb}KB"] = {"ms": ms, "GB/s": gbs, "frac_of_hbm": gbs / hbm_peak,
-                                       "marks_per_s": marks[logn] / (ms / 1e3)}
+            nc, nw = sieve_marks(n, kb * 1024)
+            row["tiles"][f"{kb}KB"] = {"ms": ms, "GB/s": gbs, "frac_of_hbm": gbs / hbm,
+                                       "marks_per_s": (nc + nw) / (ms / 1e3)}
         best = max(row["tiles"].items(), key=lambda kv: kv[1]["GB/s"])
         row["best"] = {"tile": best[0], **best[1]}
+        if not args.no_cpu_baseline:
+            row["cpu"] = cpu_segment_fill(n)
         out.append(row)
         del d
-    return {"workload": "prime map for values up to N (host prime list to sqrt N, sieve only); "
+    assert ffb.take_errors(dev) == 0
+    return {"workload": "prime map for values up to N (list made on the device, sieve only); "
                         "a 2^24 or 2^28 map fits in L2, so only the 2^32 line is HBM-sized; "
                         "host launch overhead included (one call per sieve)", "rows": out}
+
+
+def cpu_segment_fill(n):
+    """The restated SegmentFill (oracle ffo_build_map: the map of values 0..n in byte-aligned
+    chunks, one per thread) on all host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ffo
+    threads = os.cpu_count() or 1
+    ffo.build_map(min(n, 1 << 20), threads=threads)   # warm-up
+    t = time.perf_counter()
+    ffo.build_map(n, threads=threads)
+    s = time.perf_counter() - t
+    nbytes = (n + 1 + 15) >> 4
+    return {"s": s, "GB/s": nbytes / s / 1e9, "cores": threads, "kind": "port"}
 
 
 # ---------------------------------------------------------------------------------------
@@ -439,24 +679,26 @@ def served_section(args, dev):
     lib = ffb.load()
     n = args.served_requests
     budget = 8 << 30
-    base = workloads.served_requests(seed=1, n=10000, rate=1.0)[:n]
-    # capacity: the whole prefix at once
+    stream = workloads.served_requests(seed=1, n=10000, rate=1.0)
+    base = stream[:n]
+    # capacity: the first n requests at once
     sat = serve_stream(ffb, dev, [(0.0, a, b) for _, a, b in base], budget)
     cap_rps = sat["requests_per_s"]
-    # the same at a budget whose backing holds every probe of sums up to 2^22 (no
-    # Miller-Rabin): what the 8 GiB cap costs
-    full_budget = (((lib.ffb_probe_bound(1 << 22) + 1) >> 4) + (1 << 20) + (1 << 30) + (64 << 20))
-    full_budget = (full_budget + (1 << 30) - 1) >> 30 << 30
-    sat_full = serve_stream(ffb, dev, [(0.0, a, b) for _, a, b in base], full_budget)
+    # offered loads on a prefix: the seed-1 arrival gaps rescaled to a fraction of capacity
+    pre = stream[:min(n, args.served_load_requests)]
     runs = []
     for frac in args.served_loads:
         rate = frac * cap_rps
-        # the same requests, arrival gaps of the seed-1 stream rescaled to this rate
-        reqs = [(t / rate, a, b) for t, a, b in base]
+        reqs = [(t / rate, a, b) for t, a, b in pre]
         r = serve_stream(ffb, dev, reqs, budget)
         r["rate_per_s"] = rate
         r["load"] = frac
         runs.append(r)
+    # the same prefix at a budget whose backing holds every probe of sums up to 2^22 (no
+    # Miller-Rabin): what the 8 GiB cap costs
+    full_budget = (((lib.ffb_probe_bound(1 << 22) + 1) >> 4) + (1 << 20) + (1 << 30) + (64 << 20))
+    full_budget = (full_budget + (1 << 30) - 1) >> 30 << 30
+    sat_full = serve_stream(ffb, dev, [(0.0, a, b) for _, a, b in pre], full_budget)
     # the plain method once per request (ffb_run: its own map sieved, then the search)
     ctx = lib.ffb_context_create(dev)
     k = max(1, n // args.served_plain)
@@ -484,36 +726,36 @@ def served_section(args, dev):
     # every k-th request in arrival order, unbiased for the per-request mean time
     plain_total_s = plain_t * len(base) / len(sample)
     plain = sat["sums"] / plain_total_s
-    sat_full_vs_plain = sat_full["value"] / plain
-    return {"workload": f"first {n} of the 10,000 seed-1 requests (limit U{{69..2^22}}, "
-                        f"length floor(2^U[6,20]), start max(5, limit-length+1)); Poisson "
-                        f"arrivals of the seed-1 stream rescaled to each rate",
-            "budget": "8 GiB (computeBudget: f 0.90, cap 8 GiB)",
-            "saturation": sat, "rates": runs,
-            "saturation_full_map": {**{k: sat_full[k] for k in (
-                "value", "requests_per_s", "span_s", "latency_ms", "map_bytes", "map_max_value",
-                "budget_bytes", "mr_candidates")}},
-            "plain_one_launch_per_request": {
-                "value": plain, "unit": UNIT, "latency_ms_p50": pct(plain_lat, 0.5),
-                "est_total_s": plain_total_s, "sample_sums_per_s": plain_sums / plain_t,
-                "sample": f"every {n // len(sample)}th of the {n} requests ({len(sample)}), one "
-                          f"ffb_run each; the mix's time = mean time per request x {n}"},
-            "vs_plain": sat["value"] / plain, "full_map_vs_plain": sat_full_vs_plain}
+    out = {"workload": f"first {n} of the 10,000 seed-1 requests (limit U{{69..2^22}}, "
+                       f"length floor(2^U[6,20]), start max(5, limit-length+1)) submitted at "
+                       f"once (saturation); offered loads and the full-map budget on the first "
+                       f"{len(pre)}, Poisson arrivals of the seed-1 stream rescaled to each rate",
+           "budget": "8 GiB (computeBudget: f 0.90, cap 8 GiB)",
+           "saturation": sat, "rates": runs,
+           "saturation_full_map": {**{k: sat_full[k] for k in (
+               "requests", "value", "requests_per_s", "span_s", "latency_ms", "map_bytes",
+               "map_max_value", "budget_bytes", "mr_candidates")}},
+           "plain_one_launch_per_request": {
+               "value": plain, "unit": UNIT, "latency_ms_p50": pct(plain_lat, 0.5),
+               "est_total_s": plain_total_s, "sample_sums_per_s": plain_sums / plain_t,
+               "sample": f"every {k}th of the {n} requests ({len(sample)}), one ffb_run each; "
+                         f"the mix's time = mean time per request x {n}"},
+           "vs_plain": sat["value"] / plain}
+    if not args.no_cpu_baseline:
+        cpu = oracle_union_rate([(a, b) for _, a, b in base])
+        cpu["value_requested"] = sat["sums"] / cpu["est_union_s"]
+        out["cpu_baseline"] = {**cpu, "value": cpu["value_requested"], "unit": "requested sums/s"}
+        out["vs_cpu"] = sat["value"] / cpu["value_requested"]
+    return out
 
 
 # ---------------------------------------------------------------------------------------
 # the reference's CPU program
 # ---------------------------------------------------------------------------------------
-def ref_binary():
-    """ff_seg built from the reference source with the largest THREADS <= cores-1."""
-    cores = os.cpu_count() or 1
-    best, best_t = None, 0
-    for t in (31, 63, 127, 255):
-        exe = os.path.join(ROOT, "oracle", "_ref", "ff_seg" if t == 31 else f"ff_seg_t{t}")
-        if os.path.exists(exe) and (t <= cores - 1 or best is None):
-            if t > best_t:
-                best, best_t = exe, t
-    return best, best_t
+def ref_binary(threads=31):
+    """ff_seg built from the reference source with THREADS = `threads` (oracle/_ref)."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "ff_seg" if threads == 31 else f"ff_seg_t{threads}")
+    return exe if os.path.exists(exe) else None
 
 
 # The sample: 8192 odd sums around 0.505 * 2^21, where the per-sum search cost equals the
@@ -537,13 +779,12 @@ def run_ff_seg(exe, lo, hi):
 
 
 def map_bytes_for(limit):
-    import math
     mgp = (limit + 1) >> 1
     size = (max(((mgp * mgp) >> 2) + 2, 2) + 15) >> 4
     return size
 
 
-def ref_sample_value(exe, threads):
+def ref_sample_value(exe):
     lo, hi = SAMPLE
     p_us, f_us, _ = run_ff_seg(exe, lo, hi)
     n = odd_sums(lo, hi)
@@ -555,36 +796,44 @@ def ref_sample_value(exe, threads):
 
 
 def cpu_baseline(args):
-    exe, threads = ref_binary()
+    exe = ref_binary(31)
     if not exe:
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                 "sample": "reference binary not built (oracle/_ref)"}
-    v, info = ref_sample_value(exe, threads)
-    return {"value": v, "unit": UNIT, "cores": min(threads, os.cpu_count() or threads),
-            "threads": threads, "host_cores": os.cpu_count(), "kind": "reference",
-            "sample": f"ff_seg (THREADS={threads}) on odd sums {SAMPLE[0]}..{SAMPLE[1]} "
-                      f"(8192 sums of average cost); its sieve time scaled to the 2^21 map and "
-                      f"charged per sum", **info}
+    cores = os.cpu_count() or 1
+    v, info = ref_sample_value(exe)
+    out = {"value": v, "unit": UNIT, "cores": min(31, cores), "threads": 31, "host_cores": cores,
+           "kind": "reference",
+           "sample": f"ff_seg (THREADS=31, the reference's default) on odd sums {SAMPLE[0]}.."
+                     f"{SAMPLE[1]} (8192 sums of average cost); its sieve time scaled to the "
+                     f"2^21 map and charged per sum", **info}
+    t = cores - 1
+    exe_t = ref_binary(t)
+    if exe_t and t != 31:
+        v2, info2 = ref_sample_value(exe_t)
+        out["threads_nproc_minus_1"] = {"value": v2, "threads": t, **info2}
+    return out
 
 
 def reference_arm(args, rank):
     if rank != 0:
         return
-    exe, threads = ref_binary()
+    exe = ref_binary(31)
     if not exe:
         print(json.dumps({"impl": "reference", "unavailable": "reference binary oracle/_ref/ff_seg "
                                                                "not built (needs the reference checkout)"}))
         return
     vals, infos = [], []
     for _ in range(args.warmup):
-        ref_sample_value(exe, threads)
+        ref_sample_value(exe)
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        v, info = ref_sample_value(exe, threads)
+        v, info = ref_sample_value(exe)
         vals.append(v)
         infos.append(info)
     wall = time.perf_counter() - t0
     value = statistics.mean(vals)
+    cores = os.cpu_count() or 1
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * wall / args.steps,
@@ -592,9 +841,9 @@ def reference_arm(args, rank):
         "dtype": "u32/u64 integer", "data": "synthetic",
         "config": {"workload": "ff_sieve 5 2097152 (bounded sample)", "sum_start": 5,
                    "sum_limit": LIMIT},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(threads, os.cpu_count() or threads),
-                         "threads": threads, "host_cores": os.cpu_count(), "kind": "reference",
-                         "sample": f"ff_seg (THREADS={threads}, reference source) on odd sums "
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": min(31, cores),
+                         "threads": 31, "host_cores": cores, "kind": "reference",
+                         "sample": f"ff_seg (THREADS=31, reference source) on odd sums "
                                    f"{SAMPLE[0]}..{SAMPLE[1]}; sieve time scaled to the 2^21 map "
                                    f"and charged per sum", "last": infos[-1]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -612,8 +861,11 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the public-call timing")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-mode section")
     ap.add_argument("--no-sieve-sweep", action="store_true", help="skip the sieve sweep section")
-    ap.add_argument("--served-requests", type=int, default=300,
-                    help="requests of the seed-1 served stream to replay (0: skip)")
+    ap.add_argument("--served-requests", type=int, default=1000,
+                    help="requests of the seed-1 served stream replayed at saturation (0: skip; "
+                         "10000: the whole stream)")
+    ap.add_argument("--served-load-requests", type=int, default=300,
+                    help="requests of the stream replayed at each offered load")
     ap.add_argument("--served-loads", type=lambda v: [float(x) for x in v.split(",")],
                     default=[0.5, 0.8], help="offered loads, as fractions of the measured capacity")
     ap.add_argument("--served-plain", type=int, default=16,

@@ -8,8 +8,9 @@
 //     to ONE persistent search launch as its work queue (largest sums first), each sum
 //     evaluated once however many ranges share it;
 //   * the sieve and the search launches captured once into a CUDA graph and replayed;
-//   * the sieve's tile size and the search's block size picked by a small autotuner that
-//     times the candidates on the batch itself.
+//   * the sieve's tile size, the search's block size (warps per block) and the sums a warp
+//     takes per pull of the work queue (sums per chunk; sums per block = warps x chunk)
+//     picked by a small autotuner that times the candidates on the batch itself.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -41,7 +42,7 @@ struct Interval {
 };
 
 struct Tuned {
-    uint32_t tile_bytes, warps;
+    uint32_t tile_bytes, warps, chunk;
 };
 std::mutex g_tune_mu;
 std::map<std::pair<uint64_t, uint64_t>, Tuned> g_tuned;  // (map bytes, sums) -> choice
@@ -59,7 +60,7 @@ struct FfbBatch {
     std::vector<uint64_t> rec_base;  // per interval (ascending order)
     uint64_t nrec = 0;
     uint64_t map_mpv = 0, map_bytes = 0;
-    uint32_t tile_bytes = 0, warps = 8;
+    uint32_t tile_bytes = 0, warps = 8, chunk = 32;
     int tuned = 0;
     // device
     uint8_t* d_map = nullptr;
@@ -68,7 +69,6 @@ struct FfbBatch {
     uint32_t nseg = 0, nchunks = 0;
     uint32_t* d_words = nullptr;  // [0] work counter, [1] error flags
     SievePlan* sieve = nullptr;
-    std::vector<uint32_t> primes;
     cudaStream_t stream = nullptr;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
@@ -86,11 +86,10 @@ int build_sieve(FfbBatch* b)
     a.out = b->d_map;
     a.seg_lo = 0;
     a.seg_hi = b->map_mpv + 1;
-    a.h_primes = b->primes.data();
-    a.nprimes = (uint32_t)b->primes.size();
     a.tile_bytes = b->tile_bytes;
     a.clear_one = 1;
-    b->sieve = create_sieve_plan(a, b->sms);
+    a.true_map = 1;
+    b->sieve = create_sieve_plan(a, b->sms, b->d_words + 1);
     return b->sieve ? 0 : -1;
 }
 
@@ -115,7 +114,26 @@ SearchArgs search_args(const FfbBatch* b, const DeviceState* s)
     a.nseg = b->nseg;
     a.nchunks = b->nchunks;
     a.warps = b->warps;
+    a.chunk = b->chunk;
     return a;
+}
+
+// The work queue for b->chunk sums per chunk: the intervals largest first, each entry
+// {lo, count, record base, first chunk}, uploaded to d_seg (synchronously).
+int build_queue(FfbBatch* b)
+{
+    std::vector<uint4> seg;
+    b->nchunks = 0;
+    for (size_t k = b->iv.size(); k-- > 0;) {
+        const Interval& x = b->iv[k];
+        const uint32_t cnt = (x.hi - x.lo) / 2 + 1;
+        seg.push_back(make_uint4(x.lo, cnt, (uint32_t)b->rec_base[k], b->nchunks));
+        b->nchunks += (cnt + b->chunk - 1) / b->chunk;
+    }
+    b->nseg = (uint32_t)seg.size();
+    if (!seg.empty())
+        FFB_CUDA(cudaMemcpy(b->d_seg, seg.data(), sizeof(uint4) * seg.size(), cudaMemcpyHostToDevice));
+    return 0;
 }
 
 // sieve + search on b->stream, for capture: the events are recorded as nodes of the graph
@@ -152,8 +170,9 @@ int autotune(FfbBatch* b)
         if (it != g_tuned.end()) {
             b->tile_bytes = it->second.tile_bytes;
             b->warps = it->second.warps;
+            b->chunk = it->second.chunk;
             b->tuned = 2;
-            return build_sieve(b);
+            return build_queue(b) || build_sieve(b);
         }
     }
     // the tile shares the CTA's 227 KB of shared memory with ~7 KB of pre-sieve patterns
@@ -179,21 +198,27 @@ int autotune(FfbBatch* b)
     DeviceState* s = device_state(b->dev);
     if (!s) return -1;
     best = 1e30f;
-    uint32_t best_w = 8;
-    for (uint32_t w : {4u, 8u, 16u}) {
-        b->warps = w;
-        FFB_CUDA(cudaMemsetAsync(b->d_words, 0, 8, b->stream));
-        FFB_CUDA(cudaEventRecord(b->ev[1], b->stream));
-        if (b->nseg && launch_search(search_args(b, s), b->sms, b->stream)) return -1;
-        FFB_CUDA(cudaEventRecord(b->ev[2], b->stream));
-        FFB_CUDA(cudaStreamSynchronize(b->stream));
-        const float ms = elapsed(b->ev[1], b->ev[2]);
-        if (ms < best) { best = ms; best_w = w; }
+    uint32_t best_w = 8, best_c = 32;
+    for (uint32_t c : {16u, 32u, 64u}) {
+        b->chunk = c;
+        if (build_queue(b)) return -1;
+        for (uint32_t w : {4u, 8u, 16u}) {
+            b->warps = w;
+            FFB_CUDA(cudaMemsetAsync(b->d_words, 0, 8, b->stream));
+            FFB_CUDA(cudaEventRecord(b->ev[1], b->stream));
+            if (b->nseg && launch_search(search_args(b, s), b->sms, b->stream)) return -1;
+            FFB_CUDA(cudaEventRecord(b->ev[2], b->stream));
+            FFB_CUDA(cudaStreamSynchronize(b->stream));
+            const float ms = elapsed(b->ev[1], b->ev[2]);
+            if (ms < best) { best = ms; best_w = w; best_c = c; }
+        }
     }
     b->warps = best_w;
+    b->chunk = best_c;
+    if (build_queue(b)) return -1;
     b->tuned = 1;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tuned[key] = {b->tile_bytes, b->warps};
+    g_tuned[key] = {b->tile_bytes, b->warps, b->chunk};
     return 0;
 }
 
@@ -316,33 +341,19 @@ extern "C" FfbBatch* ffb_batch_create(int deviceIndex, uint32_t n, const int32_t
         b->rec_base.push_back(b->nrec);
         b->nrec += (x.hi - x.lo) / 2 + 1;
     }
-    // work queue: intervals largest first, chunks of 32 sums
-    std::vector<uint4> seg;
-    for (size_t k = b->iv.size(); k-- > 0;) {
-        const Interval& x = b->iv[k];
-        const uint32_t cnt = (x.hi - x.lo) / 2 + 1;
-        seg.push_back(make_uint4(x.lo, cnt, (uint32_t)b->rec_base[k], b->nchunks));
-        b->nchunks += (cnt + 31) / 32;
-    }
-    b->nseg = (uint32_t)seg.size();
     b->map_mpv = std::max<uint64_t>(ffb_probe_bound(std::max(top, 5u)), 15);
     b->map_bytes = (b->map_mpv + 1 + 15) >> 4;
-    uint32_t* pr = nullptr;
-    uint32_t npr = 0;
-    host_odd_primes(isqrt_u64(b->map_mpv), &pr, &npr);
-    b->primes.assign(pr, pr + npr);
-    std::free(pr);
     // ---- device buffers ----
     bool ok = cudaSetDevice(deviceIndex) == cudaSuccess &&
               cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) == cudaSuccess &&
               cudaMalloc(&b->d_map, (b->map_bytes + 255) & ~255ull) == cudaSuccess &&
               cudaMalloc(&b->d_rec, 8 * std::max<uint64_t>(b->nrec, 1)) == cudaSuccess &&
-              cudaMalloc(&b->d_seg, sizeof(uint4) * std::max<size_t>(seg.size(), 1)) == cudaSuccess &&
+              cudaMalloc(&b->d_seg, sizeof(uint4) * std::max<size_t>(b->iv.size(), 1)) == cudaSuccess &&
               cudaMalloc(&b->d_words, 256) == cudaSuccess &&
               cudaMallocHost(&b->h_rec, 8 * std::max<uint64_t>(b->nrec, 1)) == cudaSuccess;
     for (cudaEvent_t& e : b->ev) ok = ok && cudaEventCreate(&e) == cudaSuccess;
-    ok = ok && (seg.empty() || cudaMemcpy(b->d_seg, seg.data(), sizeof(uint4) * seg.size(),
-                                          cudaMemcpyHostToDevice) == cudaSuccess);
+    b->chunk = 32;
+    ok = ok && build_queue(b) == 0;
     if (!ok) {
         std::fprintf(stderr, "ffb_batch: device allocation failed (map %llu bytes): %s\n",
                      (unsigned long long)b->map_bytes, cudaGetErrorString(cudaGetLastError()));
@@ -421,6 +432,7 @@ extern "C" int ffb_batch_info(const FfbBatch* b, FfbBatchInfo* info)
     info->mapBytes = b->map_bytes;
     info->sieveTileBytes = b->tile_bytes;
     info->searchWarps = b->warps;
+    info->searchChunk = b->chunk;
     info->autotuned = b->tuned;
     info->sieveMs = 0;
     info->searchMs = 0;

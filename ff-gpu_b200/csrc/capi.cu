@@ -141,8 +141,26 @@ int run_sieve(int dev, const uint32_t* h_primes, uint32_t n, uint64_t seg_lo, ui
     a.nprimes = n;
     a.tile_bytes = tile_bytes;
     a.clear_one = clear_one;
-    return launch_sieve(a, s->sms, stream);
+    return launch_sieve(a, s->sms, err_word(s), stream);
 }
+
+int run_sieve_map(int dev, uint64_t seg_lo, uint64_t seg_hi, uint8_t* d_out, cudaStream_t stream,
+                  int clear_one, uint32_t tile_bytes)
+{
+    DeviceState* s = device_state(dev);
+    if (!s) return -1;
+    FFB_CUDA(cudaSetDevice(dev));
+    SieveArgs a;
+    a.out = d_out;
+    a.seg_lo = seg_lo;
+    a.seg_hi = seg_hi;
+    a.tile_bytes = tile_bytes;
+    a.clear_one = clear_one;
+    a.true_map = 1;
+    return launch_sieve(a, s->sms, err_word(s), stream);
+}
+
+uint32_t* device_err_word(DeviceState* s) { return err_word(s); }
 
 }  // namespace ffb
 
@@ -451,12 +469,19 @@ extern "C" int GpuSearchLaunch(int deviceIndex, const char* vendor, const uint8_
 // ---------------------------------------------------------------------------------------
 extern "C" int ffb_sieve_map_async(int deviceIndex, uint64_t mpv, uint8_t* d_map, void* stream)
 {
-    uint32_t* pr = nullptr;
-    uint32_t n = 0;
-    host_odd_primes(isqrt_u64(mpv), &pr, &n);
-    int rc = run_sieve(deviceIndex, pr, n, 0, mpv + 1, d_map, (cudaStream_t)stream, 1);
-    std::free(pr);
-    return rc;
+    return run_sieve_map(deviceIndex, 0, mpv + 1, d_map, (cudaStream_t)stream, 1);
+}
+
+extern "C" int ffb_sieve_map_range_async(int deviceIndex, uint64_t segLo, uint64_t segHi,
+                                         uint8_t* d_out, void* stream)
+{
+    if (segLo & 255) {
+        std::fprintf(stderr, "ffb_sieve_map_range_async: segLo %llu is not a multiple of 256\n",
+                     (unsigned long long)segLo);
+        return -1;
+    }
+    if (segHi <= segLo) return 0;
+    return run_sieve_map(deviceIndex, segLo, segHi, d_out, (cudaStream_t)stream, segLo == 0);
 }
 
 extern "C" int ffb_sieve_map_tiled_async(int deviceIndex, uint64_t mpv, uint8_t* d_map,
@@ -467,12 +492,7 @@ extern "C" int ffb_sieve_map_tiled_async(int deviceIndex, uint64_t mpv, uint8_t*
                      "(multiple of 16)\n", tileBytes);
         return -1;
     }
-    uint32_t* pr = nullptr;
-    uint32_t n = 0;
-    host_odd_primes(isqrt_u64(mpv), &pr, &n);
-    int rc = run_sieve(deviceIndex, pr, n, 0, mpv + 1, d_map, (cudaStream_t)stream, 1, tileBytes);
-    std::free(pr);
-    return rc;
+    return run_sieve_map(deviceIndex, 0, mpv + 1, d_map, (cudaStream_t)stream, 1, tileBytes);
 }
 
 extern "C" int ffb_search_async(int deviceIndex, const uint8_t* d_map, uint64_t mapBound,

@@ -26,14 +26,15 @@ struct SearchArgs {
     uint32_t* gcount;       // reference solution counter (or null)
     const TDiv* tdiv;       // odd primes below 65536 with exact-division constants
     uint32_t ntdiv;
-    uint32_t* sched;        // [0]: next chunk of 32 sums (must be 0 at launch)
+    uint32_t* sched;        // [0]: next chunk of sums (must be 0 at launch)
     uint32_t* err;          // error flags (ffb_device.cuh)
     unsigned long long* stats;  // [0] stage-1 probes, [1] stage-2 items (or null)
     const uint4* seg = nullptr;  // work queue of disjoint intervals {lo, count, record base, first
                             // chunk}, largest sums first (or null: the single range lo..hi)
     uint32_t nseg = 0;      // intervals in seg (0: single range)
-    uint32_t nchunks = 0;   // chunks of 32 sums over all intervals
+    uint32_t nchunks = 0;   // chunks of `chunk` sums over all intervals
     uint32_t warps = 0;     // warps per block: 4, 8 or 16 (0: 16 map-only, 8 Miller-Rabin)
+    uint32_t chunk = 32;    // sums a warp takes per pull of the work counter: 16, 32 or 64
 };
 
 // Packed per-sum record written by the search: 0 = no solution line, else
@@ -59,18 +60,21 @@ DeviceState* device_state(int device);  // nullptr (and a stderr line) on failur
 struct SieveArgs {
     uint8_t* out;            // (seg_hi - seg_lo + 15) >> 4 bytes are written
     uint64_t seg_lo, seg_hi;
-    const uint32_t* h_primes;  // marking list (host, ascending in every reference caller)
-    uint32_t nprimes;
-    uint32_t tile_bytes;       // shared-memory tile (multiple of 16; 0 = default)
-    int clear_one;             // clear the value-1 bit when seg_lo == 0 (the map init does)
+    const uint32_t* h_primes = nullptr;  // marking list (host, ascending in every reference caller)
+    uint32_t nprimes = 0;
+    uint32_t tile_bytes = 0;   // shared-memory tile (multiple of 16; 0 = default)
+    int clear_one = 0;         // clear the value-1 bit when seg_lo == 0 (the map init does)
+    int true_map = 0;          // 1: the prime map itself: the list is every odd prime p with
+                               // p*p < seg_hi, made on the device (h_primes is ignored)
 };
 
-int launch_sieve(const SieveArgs& a, int sms, cudaStream_t stream);
+// err: the device error word (a list beyond its bound raises kErrBadInput).
+int launch_sieve(const SieveArgs& a, int sms, uint32_t* err, cudaStream_t stream);
 
 // A sieve analysed once (device tables allocated and uploaded); enqueue_sieve_plan launches
 // only kernels, so it can be captured into a CUDA graph and replayed.
 struct SievePlan;
-SievePlan* create_sieve_plan(const SieveArgs& a, int sms);
+SievePlan* create_sieve_plan(const SieveArgs& a, int sms, uint32_t* err);
 int enqueue_sieve_plan(const SievePlan* p, cudaStream_t stream);
 void destroy_sieve_plan(SievePlan* p);
 int launch_search(const SearchArgs& a, int sms, cudaStream_t stream);
@@ -78,6 +82,12 @@ int launch_search(const SearchArgs& a, int sms, cudaStream_t stream);
 // Entry helpers shared by the C ABI and the pipeline (capi.cu).
 int run_sieve(int dev, const uint32_t* h_primes, uint32_t n, uint64_t seg_lo, uint64_t seg_hi,
               uint8_t* d_out, cudaStream_t stream, int clear_one, uint32_t tile_bytes = 0);
+// The prime map's values [seg_lo, seg_hi) (every odd prime p with p*p < seg_hi marks; the list
+// is made on the device) into d_out, seg_lo-relative.
+int run_sieve_map(int dev, uint64_t seg_lo, uint64_t seg_hi, uint8_t* d_out, cudaStream_t stream,
+                  int clear_one, uint32_t tile_bytes = 0);
+// The device's error word (kErr* flags, read and cleared by ffb_take_errors).
+uint32_t* device_err_word(DeviceState* s);
 int run_search(int dev, const uint8_t* d_map, uint64_t bound, uint32_t lo, uint32_t hi,
                uint64_t* d_rec, void* grec, uint32_t grec_base, uint32_t* gcount,
                cudaStream_t stream);

@@ -72,11 +72,15 @@ uint64_t fit_map_mpv(FfbContext* c, uint64_t want, uint64_t nrec)
         cudaGetLastError();
         free_b = 0;
     }
-    // the context's own buffers are freed and made again when they must grow
-    const uint64_t own = c->map_cap + 8 * c->rec_cap;
+    // Memory grow() can reuse: the map buffer (freed when the new map is larger; a map that
+    // fits in it needs nothing new) and the record buffer only when the job's records do not
+    // fit in it (grow() keeps it otherwise, and then the records need nothing new).
+    const bool rec_grows = nrec > c->rec_cap;
+    const uint64_t own = c->map_cap + (rec_grows ? 8 * c->rec_cap : 0);
     FfbBudget b{};
     ffb_compute_budget(free_b + own, 0.90, 0, 0, 0, &b);
-    uint64_t avail = b.backing > 16 * nrec ? b.backing - 16 * nrec : 0;
+    const uint64_t rec_need = rec_grows ? 16 * nrec : 0;
+    uint64_t avail = b.backing > rec_need ? b.backing - rec_need : 0;
     if (c->map_budget && c->map_budget < avail) avail = c->map_budget;
     const uint64_t want_bytes = (want + 1 + 15) >> 4;
     if (want_bytes + 256 <= avail) return want;

@@ -28,12 +28,14 @@ namespace ffb {
 namespace {
 
 constexpr int kQueue = 64;       // per-warp queue capacity (entries)
-constexpr int kMaxPf = 16;       // distinct odd prime factors of a product < 2^52
-constexpr int kMaxDiv = 64;      // divisor list of one AllButOne... call
+constexpr int kMaxPf = 12;       // distinct odd primes of a product < 2^48 (3*5*...*41 = 1.5e14)
+constexpr int kMaxDiv = 64;      // pending probes of one AllButOne... call (Miller-Rabin variant)
+constexpr uint32_t kPfMask = (1u << 26) - 1;
 
+// Prime factorisation of an odd product: factor q (below 2^26) and exponent e packed as
+// q | e << 26, in the order found.
 struct Fac {
-    uint32_t q[kMaxPf];
-    uint32_t e[kMaxPf];
+    uint32_t pf[kMaxPf];
     int n;
 };
 
@@ -80,15 +82,26 @@ __device__ __forceinline__ int pair_class(const SearchArgs& A, uint64_t i)
     return above_map_class(n, A.err);
 }
 
-// Ascending prime factorisation of an odd x < 2^32 by the exact-division table, with the
-// cofactor's primality read from the bitmap after every factor found.
-template <bool kMR>
-__device__ int factor_odd(uint32_t x, uint32_t* q, uint32_t* e, int cap, const SearchArgs& A)
+// Adds q^e to the factorisation (exponents of a prime met twice add up).
+__device__ __forceinline__ void fac_add(Fac& f, uint32_t q, uint32_t e, const SearchArgs& A)
 {
-    int cnt = 0;
+    for (int j = 0; j < f.n; ++j)
+        if ((f.pf[j] & kPfMask) == q) {
+            f.pf[j] += e << 26;
+            return;
+        }
+    if (f.n < kMaxPf) f.pf[f.n++] = q | e << 26;
+    else atomicOr(A.err, kErrFactorList);
+}
+
+// The prime factors of an odd x < 2^26 added to f: trial division by the exact-division
+// table, the cofactor's primality read from the bitmap after every factor found.
+template <bool kMR>
+__device__ void factor_into(uint32_t x, Fac& f, const SearchArgs& A)
+{
     uint32_t n = x;
-    if (n <= 1) return 0;
-    if (isp<kMR>(A, n)) { q[0] = n; e[0] = 1; return 1; }
+    if (n <= 1) return;
+    if (isp<kMR>(A, n)) { fac_add(f, n, 1, A); return; }
     for (uint32_t i = 0; i < A.ntdiv; ++i) {
         const TDiv t = A.tdiv[i];
         if ((uint64_t)t.p * t.p > n) break;
@@ -96,183 +109,115 @@ __device__ int factor_odd(uint32_t x, uint32_t* q, uint32_t* e, int cap, const S
         if (y <= t.lim) {
             uint32_t ex = 0;
             do { n = y; ++ex; y = n * t.inv; } while (y <= t.lim);
-            if (cnt < cap) { q[cnt] = t.p; e[cnt] = ex; }
-            ++cnt;
-            if (n == 1) return cnt;
-            if (isp<kMR>(A, n)) {
-                if (cnt < cap) { q[cnt] = n; e[cnt] = 1; }
-                return cnt + 1;
-            }
+            fac_add(f, t.p, ex, A);
+            if (n == 1) return;
+            if (isp<kMR>(A, n)) { fac_add(f, n, 1, A); return; }
         }
     }
-    if (n > 1) {
-        if (cnt < cap) { q[cnt] = n; e[cnt] = 1; }
-        ++cnt;
-    }
-    return cnt;
-}
-
-template <bool kMR>
-__device__ void factor_product(uint32_t a, uint32_t b, Fac& f, const SearchArgs& A)
-{
-    uint32_t qa[10], ea[10], qb[10], eb[10];
-    int na = factor_odd<kMR>(a, qa, ea, 10, A);
-    int nb = b == 1 ? 0 : factor_odd<kMR>(b, qb, eb, 10, A);
-    int i = 0, j = 0, n = 0;
-    while (i < na || j < nb) {
-        uint32_t q, e;
-        if (j >= nb || (i < na && qa[i] < qb[j])) { q = qa[i]; e = ea[i]; ++i; }
-        else if (i >= na || qb[j] < qa[i]) { q = qb[j]; e = eb[j]; ++j; }
-        else { q = qa[i]; e = ea[i] + eb[j]; ++i; ++j; }
-        if (n < kMaxPf) { f.q[n] = q; f.e[n] = e; }
-        ++n;
-    }
-    f.n = n < kMaxPf ? n : kMaxPf;
+    if (n > 1) fac_add(f, n, 1, A);
 }
 
 // AllButOneProductOfTermPairsOfSumOfFactorPairsHasSingleFactorPair
-// (reference/segmentedSieve.C:424-477) replayed from the factorisation f of oddProduct.
-// F[i] are the divisors the reference stores in factors[], C[i] = product / F[i].
+// (reference/segmentedSieve.C:424-477). The reference walks trial divisors and keeps the
+// divisors found in factors[]; the pairs it tests are exactly (d, P/d) for the odd divisors
+// 1 < d <= lim of oddProduct and (2^k d, P/(2^k d)) for the odd divisors d with 2^k d <= lim
+// (lim = isqrt(P), P = oddProduct * 2^k): its skip over sorted runs (:451) and its early
+// breaks only leave out divisors above lim. The verdict is "exactly one of those pairs is not
+// single", and the reference returns early only once two are found, so the order of the
+// tests does not matter. Here the odd divisors <= lim are enumerated from the factorisation
+// with an odometer over the exponents (digit i counts the power of factor i, 5 bits each; a
+// digit that cannot grow without passing lim is reset and the next one grows), keeping per
+// digit the divisor made of the digits from i up; the cofactor oddProduct/d is an exact
+// double division (both below 2^53, the quotient an integer). No divisor list is stored.
 template <bool kMR>
 __device__ __noinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const Fac& f,
                                          const SearchArgs& A)
 {
     const uint64_t P = odd_product << k;
     const uint64_t lim = isqrt64(P);
-    uint64_t F[kMaxDiv], C[kMaxDiv];
-    uint32_t nf = 0, npend = 0, nm = 0;
-    F[0] = 1ull << k;
-    C[0] = odd_product;
-    if (F[0] <= lim) {
-        nm += !pair1<kMR>(A, F[0] + C[0]);
-        nf = 1;
-    }
-    int idx = 0;
-    bool first = true;  // the reference tries 3 before its first IsPrime(testProduct)
+    uint32_t nm = 0;
+    if ((1ull << k) <= lim) nm += !pair1<kMR>(A, (1ull << k) + odd_product);
+    const int n = f.n;
+    const double od = (double)odd_product;
+    uint32_t Sd[kMaxPf + 1];      // divisor of the digits i.. (at most lim < 2^26)
+    uint64_t ex = 0;              // digit values, 5 bits each
+    for (int j = 0; j <= n; ++j) Sd[j] = 1;
     for (;;) {
-        uint64_t q;
-        uint32_t e;
-        if (first) {
-            first = false;
-            if (f.n > 0 && f.q[0] == 3) { q = 3; e = f.e[0]; idx = 1; }
-            else continue;
-        } else {
-            if (idx >= f.n) break;                                   // testProduct == 1
-            q = f.q[idx];
-            e = f.e[idx];
-            if (idx == f.n - 1 && e == 1 && q > lim) break;          // prime cofactor > limit
-            ++idx;
+        int i = 0;
+        uint32_t q = 0;
+        for (; i < n; ++i) {
+            q = f.pf[i] & kPfMask;
+            const uint32_t e = f.pf[i] >> 26, a = (uint32_t)(ex >> (5 * i)) & 31;
+            if (a < e && (uint64_t)Sd[i] * q <= lim) break;
+            ex &= ~(31ull << (5 * i));
+            Sd[i] = Sd[i + 1];
         }
-        // the reference's divides-branch for q, q^2, ..., q^e
-        const uint64_t qi = inv64(q);
-        uint64_t tf = q, tfi = qi;
-        for (uint32_t j = 0; j < e; ++j) {
-            if (tf <= lim) {
-                const uint64_t ctf = (odd_product * tfi) << k;     // P / tf, exact
-                if ((nm += !pair1<kMR>(A, tf + ctf)) > 1) return false;
-                if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return false; }
-                F[nf + npend] = tf;
-                C[nf + npend] = ctf;
-                ++npend;
-                for (uint32_t g = 0; g < nf; ++g) {
-                    const uint64_t m = F[g] * tf;
-                    if (m <= lim) {
-                        const uint64_t cm = C[g] * tfi;              // C[g] / tf, exact
-                        if ((nm += !pair1<kMR>(A, m + cm)) > 1) return false;
-                        if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return false; }
-                        F[nf + npend] = m;
-                        C[nf + npend] = cm;
-                        ++npend;
-                    } else {
-                        // skip the rest of this ascending run of F (reference :451)
-                        for (const uint64_t v = F[g]; g + 1 < nf && v <= F[g + 1]; ++g) {}
-                    }
-                }
-                if (nm > 1) return false;
-            }
-            tf *= q;
-            tfi *= qi;
-        }
-        nf += npend;
-        npend = 0;
+        if (i == n) break;
+        ex += 1ull << (5 * i);
+        const uint32_t d = Sd[i] * q;
+        for (int j = 0; j <= i; ++j) Sd[j] = d;
+        const uint64_t c = (uint64_t)__ddiv_rn(od, (double)d);   // odd_product / d, exact
+        if ((nm += !pair1<kMR>(A, d + (c << k))) > 1) return false;
+        if (((uint64_t)d << k) <= lim && (nm += !pair1<kMR>(A, ((uint64_t)d << k) + c)) > 1)
+            return false;
     }
     return nm == 1;
 }
 
-// all_but_one for the Miller-Rabin variant: the same divisor pairs in the same order, but a
+// all_but_one for the Miller-Rabin variant: the same divisor pairs (same odometer), but a
 // pair sum whose probe lies above the map (and has no small factor) is appended to pend[]
 // instead of being tested here, so that the warp can test them 32 at a time. Returns the
 // count of pairs already known not to be single (2 once the verdict is "no"); the verdict is
 // "yes" iff that count plus the pending probes found composite is exactly 1 (the order of the
-// tests does not change it). *np receives the number of pending pair sums.
+// tests does not change it). *np receives the number of pending pair sums (at most kMaxDiv:
+// more raises kErrFactorList).
 __device__ __noinline__ uint32_t all_but_one_defer(uint32_t k, uint64_t odd_product, const Fac& f,
                                                    const SearchArgs& A, uint64_t* pend,
                                                    uint32_t* np)
 {
     const uint64_t P = odd_product << k;
     const uint64_t lim = isqrt64(P);
-    uint64_t F[kMaxDiv], C[kMaxDiv];
-    uint32_t nf = 0, npend = 0, nm = 0, nd = 0;
+    uint32_t nm = 0, nd = 0;
     *np = 0;
-    // counts a pair sum: 0 not single, 1 single, 2 pending; returns true once nm > 1
+    // counts a pair sum: 0 not single, 1 single, 2 pending; returns true once the verdict is
+    // "no" (nm > 1) or the pending list is full
     auto visit = [&](uint64_t v) {
         const int c = pair_class(A, v);
-        if (c == 2) pend[nd++] = v;
-        else nm += c == 0;
+        if (c == 2) {
+            if (nd >= kMaxDiv) {
+                atomicOr(A.err, kErrFactorList);
+                nm = 2;
+                return true;
+            }
+            pend[nd++] = v;
+        } else {
+            nm += c == 0;
+        }
         return nm > 1;
     };
-    F[0] = 1ull << k;
-    C[0] = odd_product;
-    if (F[0] <= lim) {
-        visit(F[0] + C[0]);
-        nf = 1;
-    }
-    int idx = 0;
-    bool first = true;  // the reference tries 3 before its first IsPrime(testProduct)
+    if ((1ull << k) <= lim && visit((1ull << k) + odd_product)) return 2;
+    const int n = f.n;
+    const double od = (double)odd_product;
+    uint32_t Sd[kMaxPf + 1];
+    uint64_t ex = 0;
+    for (int j = 0; j <= n; ++j) Sd[j] = 1;
     for (;;) {
-        uint64_t q;
-        uint32_t e;
-        if (first) {
-            first = false;
-            if (f.n > 0 && f.q[0] == 3) { q = 3; e = f.e[0]; idx = 1; }
-            else continue;
-        } else {
-            if (idx >= f.n) break;                                   // testProduct == 1
-            q = f.q[idx];
-            e = f.e[idx];
-            if (idx == f.n - 1 && e == 1 && q > lim) break;          // prime cofactor > limit
-            ++idx;
+        int i = 0;
+        uint32_t q = 0;
+        for (; i < n; ++i) {
+            q = f.pf[i] & kPfMask;
+            const uint32_t e = f.pf[i] >> 26, a = (uint32_t)(ex >> (5 * i)) & 31;
+            if (a < e && (uint64_t)Sd[i] * q <= lim) break;
+            ex &= ~(31ull << (5 * i));
+            Sd[i] = Sd[i + 1];
         }
-        const uint64_t qi = inv64(q);
-        uint64_t tf = q, tfi = qi;
-        for (uint32_t j = 0; j < e; ++j) {
-            if (tf <= lim) {
-                const uint64_t ctf = (odd_product * tfi) << k;     // P / tf, exact
-                if (visit(tf + ctf)) return 2;
-                if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return 2; }
-                F[nf + npend] = tf;
-                C[nf + npend] = ctf;
-                ++npend;
-                for (uint32_t g = 0; g < nf; ++g) {
-                    const uint64_t m = F[g] * tf;
-                    if (m <= lim) {
-                        const uint64_t cm = C[g] * tfi;              // C[g] / tf, exact
-                        if (visit(m + cm)) return 2;
-                        if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return 2; }
-                        F[nf + npend] = m;
-                        C[nf + npend] = cm;
-                        ++npend;
-                    } else {
-                        // skip the rest of this ascending run of F (reference :451)
-                        for (const uint64_t v = F[g]; g + 1 < nf && v <= F[g + 1]; ++g) {}
-                    }
-                }
-            }
-            tf *= q;
-            tfi *= qi;
-        }
-        nf += npend;
-        npend = 0;
+        if (i == n) break;
+        ex += 1ull << (5 * i);
+        const uint32_t d = Sd[i] * q;
+        for (int j = 0; j <= i; ++j) Sd[j] = d;
+        const uint64_t c = (uint64_t)__ddiv_rn(od, (double)d);   // odd_product / d, exact
+        if (visit(d + (c << k))) return 2;
+        if (((uint64_t)d << k) <= lim && visit(((uint64_t)d << k) + c)) return 2;
     }
     *np = nd;
     return nm;
@@ -294,14 +239,17 @@ __device__ bool stage2(uint32_t item, uint32_t s, const SearchArgs& A, uint32_t*
     uint64_t odd_product;
     if (item & 32) {
         const uint32_t odd = s - (1u << k);
-        factor_product<kMR>(odd, 1, f, A);
+        f.n = 0;
+        factor_into<kMR>(odd, f, A);
         odd_product = odd;
         *ta = 1u << k;
         *tb = odd;
     } else {
         const uint32_t o = item >> 6;
         const uint32_t even = o << k, b = s - even;
-        factor_product<kMR>(o, b, f, A);
+        f.n = 0;
+        factor_into<kMR>(o, f, A);
+        factor_into<kMR>(b, f, A);
         odd_product = (uint64_t)o * b;
         *ta = even;
         *tb = b;
@@ -319,14 +267,17 @@ __device__ uint32_t stage2_defer(uint32_t item, uint32_t s, const SearchArgs& A,
     uint64_t odd_product;
     if (item & 32) {
         const uint32_t odd = s - (1u << k);
-        factor_product<true>(odd, 1, f, A);
+        f.n = 0;
+        factor_into<true>(odd, f, A);
         odd_product = odd;
         *ta = 1u << k;
         *tb = odd;
     } else {
         const uint32_t o = item >> 6;
         const uint32_t even = o << k, b = s - even;
-        factor_product<true>(o, b, f, A);
+        f.n = 0;
+        factor_into<true>(o, f, A);
+        factor_into<true>(b, f, A);
         odd_product = (uint64_t)o * b;
         *ta = even;
         *tb = b;
@@ -603,24 +554,15 @@ __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
     __shared__ WarpQ<kMR> queues[W];
     const int lane = threadIdx.x & 31;
     WarpQ<kMR>& Q = queues[threadIdx.x >> 5];
-    const uint32_t nchunks = A.nseg ? A.nchunks : (A.nsums + 31) / 32;
+    const uint32_t K = A.chunk;     // sums per chunk: 16, 32 or 64
+    const uint32_t nchunks = A.nseg ? A.nchunks : (A.nsums + K - 1) / K;
     for (;;) {
         uint32_t c = 0;
         if (lane == 0) c = atomicAdd(A.sched, 1u);
         c = __shfl_sync(0xFFFFFFFFu, c, 0);
         if (c >= nchunks) break;
-
-        // ---- lane-parallel: filter + Power2Prime for 32 sums (largest first) ----
-        bool act;
-        uint32_t s = 5, ri = 0;
-        if (A.nseg == 0) {
-            const uint32_t idx = c * 32 + lane;
-            act = idx < A.nsums;
-            if (act) {
-                s = A.hi - 2 * idx;
-                ri = (s - A.lo) >> 1;
-            }
-        } else {
+        uint4 g = make_uint4(0, 0, 0, 0);
+        if (A.nseg) {
             // work queue of disjoint sum intervals, largest first: the interval whose chunks
             // contain chunk c (entries {lo, count, record base, first chunk}, ascending in .w)
             uint32_t a = 0, b = A.nseg - 1;
@@ -628,78 +570,92 @@ __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
                 const uint32_t m = (a + b + 1) >> 1;
                 if (__ldg(&A.seg[m].w) <= c) a = m; else b = m - 1;
             }
-            const uint4 g = __ldg(&A.seg[a]);
-            const uint32_t idx = (c - g.w) * 32 + lane;
-            act = idx < g.y;
-            if (act) {
-                s = g.x + 2 * (g.y - 1 - idx);  // descending within the interval
-                ri = g.z + ((s - g.x) >> 1);
-            }
+            g = __ldg(&A.seg[a]);
         }
-        bool surv = false;
-        uint32_t cnt = 0, ta = 0, tb = 0, comp = 0;
-        if (act) {
-            // Sammy's first statement (reference/segmentedSieve.C:805-806)
-            const uint32_t d3 = s / 3;
-            bool pass = !pair1<kMR>(A, s) &&
-                        (s != 3 * d3 || isp<kMR>(A, d3));
-            if (pass) {
-                // Power2Prime (reference/segmentedSieve.C:547-564)
-                for (uint32_t even = 4, k = 2; even < s - 2; even <<= 1, ++k) {
-                    const uint32_t odd = s - even;
-                    if (isp<kMR>(A, odd)) {
-                        if (++cnt > 1) break;
-                        if (cnt == 1) { ta = even; tb = odd; }
-                    } else {
-                        comp |= 1u << k;
-                    }
+        for (uint32_t h = 0; h < K; h += 32) {
+            // ---- lane-parallel: filter + Power2Prime for up to 32 sums (largest first) ----
+            bool act = h + lane < K;
+            uint32_t s = 5, ri = 0;
+            if (A.nseg == 0) {
+                const uint32_t idx = c * K + h + lane;
+                act = act && idx < A.nsums;
+                if (act) {
+                    s = A.hi - 2 * idx;
+                    ri = (s - A.lo) >> 1;
                 }
-                surv = cnt <= 1;
-            }
-        }
-
-        // ---- warp-cooperative: the remaining phases, one survivor at a time ----
-        uint32_t smask = __ballot_sync(0xFFFFFFFFu, surv);
-        while (smask) {
-            const int src = __ffs(smask) - 1;
-            smask &= smask - 1;
-            SumState st;
-            st.s = __shfl_sync(0xFFFFFFFFu, s, src);
-            const uint32_t sri = __shfl_sync(0xFFFFFFFFu, ri, src);
-            st.count = __shfl_sync(0xFFFFFFFFu, cnt, src);
-            st.ta = __shfl_sync(0xFFFFFFFFu, ta, src);
-            st.tb = __shfl_sync(0xFFFFFFFFu, tb, src);
-            const uint32_t cmask = __shfl_sync(0xFFFFFFFFu, comp, src);
-            st.na = 0;
-            st.nb = 0;
-            st.nc = 0;
-            // Power2Composite items (reference/segmentedSieve.C:591-605) go straight to stage 2
-            st.nb = push(Q.b, 0, (cmask >> lane) & 1, enc(lane, 0, true), lane);
-            bool open = true;
-            if constexpr (kMR) {
-                if (st.nb >= 32) open = settle_mr(st, Q, A, lane, false);
-            } else if (st.nb >= 32) {
-                drain_b(st, Q, A, lane);
-                open = st.count <= 1;
-            }
-            if (open) open = run_phase<true, kMR>(st, Q, A, lane);
-            if (open) open = run_phase<false, kMR>(st, Q, A, lane);
-            // flush the partly filled queues: stage 1, then Miller-Rabin, then stage 2
-            if constexpr (kMR) {
-                if (open) open = settle_mr(st, Q, A, lane, true);
             } else {
-                while (open && st.na > 0) {
-                    drain_a(st, Q, A, lane);
-                    if (st.nb >= 32) { drain_b(st, Q, A, lane); open = st.count <= 1; }
+                const uint32_t idx = (c - g.w) * K + h + lane;
+                act = act && idx < g.y;
+                if (act) {
+                    s = g.x + 2 * (g.y - 1 - idx);  // descending within the interval
+                    ri = g.z + ((s - g.x) >> 1);
                 }
-                while (open && st.nb > 0) {
+            }
+            bool surv = false;
+            uint32_t cnt = 0, ta = 0, tb = 0, comp = 0;
+            if (act) {
+                // Sammy's first statement (reference/segmentedSieve.C:805-806)
+                const uint32_t d3 = s / 3;
+                bool pass = !pair1<kMR>(A, s) &&
+                            (s != 3 * d3 || isp<kMR>(A, d3));
+                if (pass) {
+                    // Power2Prime (reference/segmentedSieve.C:547-564)
+                    for (uint32_t even = 4, k = 2; even < s - 2; even <<= 1, ++k) {
+                        const uint32_t odd = s - even;
+                        if (isp<kMR>(A, odd)) {
+                            if (++cnt > 1) break;
+                            if (cnt == 1) { ta = even; tb = odd; }
+                        } else {
+                            comp |= 1u << k;
+                        }
+                    }
+                    surv = cnt <= 1;
+                }
+            }
+
+            // ---- warp-cooperative: the remaining phases, one survivor at a time ----
+            uint32_t smask = __ballot_sync(0xFFFFFFFFu, surv);
+            while (smask) {
+                const int src = __ffs(smask) - 1;
+                smask &= smask - 1;
+                SumState st;
+                st.s = __shfl_sync(0xFFFFFFFFu, s, src);
+                const uint32_t sri = __shfl_sync(0xFFFFFFFFu, ri, src);
+                st.count = __shfl_sync(0xFFFFFFFFu, cnt, src);
+                st.ta = __shfl_sync(0xFFFFFFFFu, ta, src);
+                st.tb = __shfl_sync(0xFFFFFFFFu, tb, src);
+                const uint32_t cmask = __shfl_sync(0xFFFFFFFFu, comp, src);
+                st.na = 0;
+                st.nb = 0;
+                st.nc = 0;
+                // Power2Composite items (reference/segmentedSieve.C:591-605) go straight to stage 2
+                st.nb = push(Q.b, 0, (cmask >> lane) & 1, enc(lane, 0, true), lane);
+                bool open = true;
+                if constexpr (kMR) {
+                    if (st.nb >= 32) open = settle_mr(st, Q, A, lane, false);
+                } else if (st.nb >= 32) {
                     drain_b(st, Q, A, lane);
                     open = st.count <= 1;
                 }
+                if (open) open = run_phase<true, kMR>(st, Q, A, lane);
+                if (open) open = run_phase<false, kMR>(st, Q, A, lane);
+                // flush the partly filled queues: stage 1, then Miller-Rabin, then stage 2
+                if constexpr (kMR) {
+                    if (open) open = settle_mr(st, Q, A, lane, true);
+                } else {
+                    while (open && st.na > 0) {
+                        drain_a(st, Q, A, lane);
+                        if (st.nb >= 32) { drain_b(st, Q, A, lane); open = st.count <= 1; }
+                    }
+                    while (open && st.nb > 0) {
+                        drain_b(st, Q, A, lane);
+                        open = st.count <= 1;
+                    }
+                }
+                if (open && st.count == 1 && lane == 0) write_result<kMR>(A, st.s, sri, st.ta, st.tb);
+                __syncwarp();
             }
-            if (open && st.count == 1 && lane == 0) write_result<kMR>(A, st.s, sri, st.ta, st.tb);
-            __syncwarp();
-        }
+        }   // rounds of the chunk
     }
 }
 
@@ -711,7 +667,7 @@ int launch_w(const SearchArgs& a, int sms, cudaStream_t stream)
     int per_sm = 0;
     FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel<W, kMR>, W * 32, 0));
     if (per_sm < 1) per_sm = 1;
-    const uint32_t chunks = a.nseg ? a.nchunks : (a.nsums + 31) / 32;
+    const uint32_t chunks = a.nseg ? a.nchunks : (a.nsums + a.chunk - 1) / a.chunk;
     uint32_t blocks = (uint32_t)sms * (uint32_t)per_sm;
     const uint32_t need = (chunks + W - 1) / W;
     if (blocks > need) blocks = need;
@@ -726,6 +682,10 @@ int launch_w(const SearchArgs& a, int sms, cudaStream_t stream)
 int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
 {
     if (a.nseg == 0 && a.nsums == 0) return 0;
+    if (a.chunk != 16 && a.chunk != 32 && a.chunk != 64) {
+        std::fprintf(stderr, "ffb: search chunk of %u sums (16, 32 or 64)\n", a.chunk);
+        return -1;
+    }
     const uint64_t pb = ffb_probe_bound(a.hi);
     const bool mr = pb == 0 || a.bound < pb;
     switch (a.warps) {

@@ -1,10 +1,10 @@
 // search_noalloc.cu -- ffb_search_noalloc: the Freudenthal search without any device
 // allocation, for callers that must not call cudaMalloc.
 //
-// The ordinary entry points keep their work counters, error flags and the trial-division
-// table in device memory allocated on first use of a GPU. This variant keeps the same
-// three things in one file-scope array compiled into the library instead, so a call only
-// memsets, launches and returns.
+// The ordinary entry points keep their work counter, error flags and the trial-division
+// table in device memory allocated on first use of a GPU. This variant keeps the counter
+// and the table in one file-scope array compiled into the library instead, and writes the
+// error flags to a word the caller passes, so a call only memsets, launches and returns.
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -18,11 +18,12 @@ namespace ffb {
 namespace {
 
 constexpr uint32_t kTablePrimes = 6541;     // the odd primes below 2^16
-constexpr size_t kTableOffset = 256;        // after the counter and the error word
+constexpr size_t kTableOffset = 256;        // after the work counter
 constexpr size_t kScratchBytes = kTableOffset + sizeof(TDiv) * kTablePrimes;  // 104,912 bytes
 constexpr int kMaxDevices = 64;
 
-// Layout: bytes [0,4) the search's work counter, [4,8) its error flags, [256, ...) the
+// Layout: bytes [0,4) the search's work counter, [4,256) unused (the error flags go to the
+// caller's word), [256, ...) the
 // exact-division table of the odd primes below 2^16. Present on every GPU that loads the
 // library, for the life of the process. Host code must not use this name as a device
 // address: the address comes from cudaGetSymbolAddress in setup() below.
@@ -91,10 +92,11 @@ extern "C" int ffb_search_noalloc(int deviceIndex, const uint8_t* d_map, uint64_
                                   uint32_t lo, uint32_t hi, uint64_t* d_rec, uint32_t* d_err,
                                   void* stream)
 {
-    if (!(lo & 1) || hi < lo || hi > kMaxSum || !d_map || !d_rec) {
+    if (!(lo & 1) || hi < lo || hi > kMaxSum || !d_map || !d_rec || !d_err) {
         std::fprintf(stderr,
                      "ffb_search_noalloc: sums [%u, %u] rejected: need an odd first sum, last >= "
-                     "first, last <= 2^25 (%u), and non-null map and record pointers\n",
+                     "first, last <= 2^25 (%u), and non-null map, record and error-word "
+                     "pointers\n",
                      lo, hi, kMaxSum);
         return -1;
     }
@@ -127,11 +129,11 @@ extern "C" int ffb_search_noalloc(int deviceIndex, const uint8_t* d_map, uint64_
     a.tdiv = reinterpret_cast<const TDiv*>(r.scratch + kTableOffset);
     a.ntdiv = kTablePrimes;
     a.sched = reinterpret_cast<uint32_t*>(r.scratch);
-    a.err = d_err ? d_err : reinterpret_cast<uint32_t*>(r.scratch + 4);
+    a.err = d_err;
     a.stats = nullptr;
     // the scratch keeps the previous call's counter: start this one from zero
     FFB_CUDA(cudaMemsetAsync(r.scratch, 0, 8, st));
-    if (d_err) FFB_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
+    FFB_CUDA(cudaMemsetAsync(d_err, 0, 4, st));
     FFB_CUDA(cudaMemsetAsync(d_rec, 0, 8ull * a.nsums, st));
     return launch_search(a, r.sms, st);
 }

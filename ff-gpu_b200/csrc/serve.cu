@@ -164,16 +164,12 @@ uint64_t map_need(const FfbServer* S, uint32_t top)
 // its global position: seg_lo is a multiple of 256, so byte seg_lo/16 is 16-byte aligned).
 int grow_map(FfbServer* S, uint64_t hi, Growth* growth)
 {
-    uint32_t* pr = nullptr;
-    uint32_t n = 0;
-    host_odd_primes(isqrt_u64(hi - 1), &pr, &n);
     Growth g;
     FFB_CUDA(cudaEventCreate(&g.a));
     FFB_CUDA(cudaEventCreate(&g.b));
     FFB_CUDA(cudaEventRecord(g.a, S->grow_stream));
     const uint64_t lo = S->sieved;
-    const int rc = run_sieve(S->dev, pr, n, lo, hi, S->d_map + (lo >> 4), S->grow_stream, lo == 0);
-    std::free(pr);
+    const int rc = run_sieve_map(S->dev, lo, hi, S->d_map + (lo >> 4), S->grow_stream, lo == 0);
     if (rc || cudaEventRecord(g.b, S->grow_stream) != cudaSuccess) {
         cudaEventDestroy(g.a);
         cudaEventDestroy(g.b);
@@ -382,8 +378,21 @@ void scheduler(FfbServer* S)
     S->cv_done.notify_all();
 }
 
-// Formats the launch's slices (completer thread, mu not held): chunks in slice order.
-void emit_launch(FfbServer* S, Slot& sl, std::vector<FfbServeChunk>& chunks)
+// What emitting one launch changes in a request's emission state; applied under mu.
+struct Emitted {
+    Request* r;
+    uint32_t lines, seq;
+    uint64_t hash, text_bytes;
+    double done_us;
+};
+
+// Formats the launch's slices (completer thread, mu not held): chunks in slice order. Only
+// the completer thread writes a request's emission state, so it reads that state here
+// without the lock; its new values go to `upd`, which the caller stores under mu (readers
+// such as ffb_serve_request_info take mu). `failed` holds, per piece, whether its request
+// had failed when the launch was taken (read under mu).
+void emit_launch(FfbServer* S, Slot& sl, const std::vector<char>& failed,
+                 std::vector<FfbServeChunk>& chunks, std::vector<Emitted>& upd)
 {
     size_t i = 0;
     char line[kMaxLine];
@@ -391,9 +400,16 @@ void emit_launch(FfbServer* S, Slot& sl, std::vector<FfbServeChunk>& chunks)
         Request* r = sl.pieces[i].r;
         size_t j = i;
         while (j < sl.pieces.size() && sl.pieces[j].r == r) ++j;
-        if (r->state < 0) { i = j; continue; }
+        if (failed[i]) { i = j; continue; }
+        Emitted* e = nullptr;
+        for (Emitted& u : upd)
+            if (u.r == r) e = &u;
+        if (!e) {
+            upd.push_back({r, r->lines, r->seq, r->hash, r->text_bytes, r->done_us});
+            e = &upd.back();
+        }
         std::string text;
-        if (r->seq == 0) text = r->header;
+        if (e->seq == 0) text = r->header;
         bool final = false;
         for (size_t k = i; k < j; ++k) {
             const Piece& p = sl.pieces[k];
@@ -402,11 +418,11 @@ void emit_launch(FfbServer* S, Slot& sl, std::vector<FfbServeChunk>& chunks)
             for (uint32_t s = p.lo; s <= p.hi; s += 2) {
                 const uint64_t v = rec[(s - p.lo) >> 1];
                 if (!v) continue;
-                char* e = format_line(line, ++r->lines, s, rec_low(v), rec_high(v),
-                                      rec_low_prime(v), rec_high_prime(v));
-                text.append(line, (size_t)(e - line));
+                char* end = format_line(line, ++e->lines, s, rec_low(v), rec_high(v),
+                                        rec_low_prime(v), rec_high_prime(v));
+                text.append(line, (size_t)(end - line));
             }
-            r->hash = fnv1a(r->hash, text.data() + body0, text.size() - body0);
+            e->hash = fnv1a(e->hash, text.data() + body0, text.size() - body0);
             final = final || p.last;
         }
         if (final) {
@@ -414,18 +430,18 @@ void emit_launch(FfbServer* S, Slot& sl, std::vector<FfbServeChunk>& chunks)
             float ms = 0;
             if (r->grow_a && cudaEventElapsedTime(&ms, r->grow_a, r->grow_b) == cudaSuccess)
                 prime_us = 1e3 * ms;
-            r->done_us = S->now_us();
+            e->done_us = S->now_us();
             char tail[160];
             const int n = std::snprintf(
                 tail, sizeof tail, "Prime time: %llu \xce\xbcs\nFreudenthal time: %llu \xce\xbcs\n",
-                (unsigned long long)prime_us, (unsigned long long)(r->done_us - r->admit_us));
+                (unsigned long long)prime_us, (unsigned long long)(e->done_us - r->admit_us));
             text.append(tail, (size_t)n);
         }
         char* buf = (char*)std::malloc(text.size() + 1);
         std::memcpy(buf, text.data(), text.size());
         buf[text.size()] = 0;
-        r->text_bytes += text.size();
-        chunks.push_back({r->id, r->seq++, final ? 1 : 0, buf, text.size()});
+        e->text_bytes += text.size();
+        chunks.push_back({r->id, e->seq++, final ? 1 : 0, buf, text.size()});
         i = j;
     }
 }
@@ -439,7 +455,10 @@ void completer(FfbServer* S)
         if (S->inflight.empty()) break;
         const int si = S->inflight.front();
         Slot& sl = S->slots[si];
+        std::vector<char> failed(sl.pieces.size());
+        for (size_t k = 0; k < sl.pieces.size(); ++k) failed[k] = sl.pieces[k].r->state < 0;
         lk.unlock();
+        std::vector<Emitted> upd;
         std::vector<FfbServeChunk> chunks;
         bool ok = sl.launched && cudaEventSynchronize(sl.done) == cudaSuccess;
         float ms = 0;
@@ -450,8 +469,15 @@ void completer(FfbServer* S)
         }
         uint64_t nsums = 0;
         for (const Piece& p : sl.pieces) nsums += (p.hi - p.lo) / 2 + 1;
-        if (ok) emit_launch(S, sl, chunks);
+        if (ok) emit_launch(S, sl, failed, chunks, upd);
         lk.lock();
+        for (const Emitted& u : upd) {
+            u.r->lines = u.lines;
+            u.r->seq = u.seq;
+            u.r->hash = u.hash;
+            u.r->text_bytes = u.text_bytes;
+            u.r->done_us = u.done_us;
+        }
         if (!ok) fail_pieces(S, sl, chunks);
         S->search_ms += ms;
         S->sums_searched += sl.nrec;

@@ -26,7 +26,8 @@ class FfbBatchInfo(ctypes.Structure):
                 ("sums", ctypes.c_uint64), ("mapMaxValue", ctypes.c_uint64),
                 ("mapBytes", ctypes.c_uint64), ("sieveTileBytes", ctypes.c_uint32),
                 ("searchWarps", ctypes.c_uint32), ("autotuned", ctypes.c_int),
-                ("sieveMs", ctypes.c_float), ("searchMs", ctypes.c_float)]
+                ("sieveMs", ctypes.c_float), ("searchMs", ctypes.c_float),
+                ("searchChunk", ctypes.c_uint32)]
 
 
 class FfbGeometry(ctypes.Structure):
@@ -54,6 +55,17 @@ class FfbServeConfig(ctypes.Structure):
 class FfbServeChunk(ctypes.Structure):
     _fields_ = [("request", ctypes.c_uint64), ("seq", ctypes.c_uint32), ("status", ctypes.c_int32),
                 ("text", ctypes.c_void_p), ("len", ctypes.c_size_t)]
+
+
+class FfbPeaks(ctypes.Structure):
+    """Measured on-chip peaks (ffb_measure_peaks), operations per second."""
+    _fields_ = [("imad32PerS", ctypes.c_double), ("alu32PerS", ctypes.c_double),
+                ("mul64PerS", ctypes.c_double), ("intOpsPerS", ctypes.c_double),
+                ("atomsConflictFreePerS", ctypes.c_double), ("atomsRandomPerS", ctypes.c_double),
+                ("smemRmwPerS", ctypes.c_double), ("sms", ctypes.c_int), ("clockMhz", ctypes.c_double)]
+
+    def as_dict(self):
+        return {n: getattr(self, n) for n, _ in self._fields_}
 
 
 class FfbServeRequestInfo(ctypes.Structure):
@@ -124,6 +136,9 @@ SIGNATURES = {
                                         ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
                                         ctypes.c_void_p]),
     "ffb_take_errors": (ctypes.c_int, [ctypes.c_int, u32p]),
+    "ffb_sieve_map_range_async": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint64,
+                                                 ctypes.c_void_p, ctypes.c_void_p]),
+    "ffb_measure_peaks": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(FfbPeaks)]),
     "ffb_probe_bound": (ctypes.c_uint64, [ctypes.c_uint32]),
     "ffb_search_stats": (ctypes.c_int, [ctypes.c_int, u64p, ctypes.c_int]),
     "ffb_search_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
@@ -416,3 +431,11 @@ class Server:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def measure_peaks(dev=0):
+    """ffb_measure_peaks as a dict (operations per second)."""
+    p = FfbPeaks()
+    if load().ffb_measure_peaks(dev, ctypes.byref(p)) != 0:
+        raise RuntimeError("ffb_measure_peaks failed")
+    return p.as_dict()

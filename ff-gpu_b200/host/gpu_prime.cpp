@@ -46,14 +46,18 @@ GpuPrime::Boolean GpuPrime::AskMillerRabin(uint64_t n) const
     return True;
 }
 
+// PrintOutputTags (source/m4/gpu_search_emission.cpp:34-50). A term of 0 (which no search
+// produces; the reference prints "(2^-inf)" for it) is treated as composite.
 void PrintOutputTags(const GpuPrime& prime, uint64_t term, bool isLast)
 {
     if (prime.IsPrime(term)) {
         std::fputs(isLast ? " (prime), " : " (prime)", stdout);
     } else if (term && (term & (term - 1)) == 0) {
+        // " (2^N)", then "," padded to width 3 - floor(log10(N + 0.001)) (at least 1): six
+        // blanks for N = 0, three for 1..9, two for 10..63
         const int n = __builtin_ctzll(term);
         std::printf(" (2^%d)", n);
-        if (isLast) std::fputs(n < 10 ? ",   " : ",  ", stdout);
+        if (isLast) std::fputs(n == 0 ? ",      " : n < 10 ? ",   " : ",  ", stdout);
     } else if (isLast) {
         std::fputs(",         ", stdout);
     }

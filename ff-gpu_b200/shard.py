@@ -1,11 +1,14 @@
 """Sharding one ff_sieve job over several GPUs (one process per GPU).
 
-The odd sums of a job are independent, so a job splits into contiguous shards, one per
-rank, with no exchange while the sums are searched: each rank sieves the map its own shard
-needs and searches it. The only collective is the gather of the packed records to rank 0,
-which then emits ff_seg's text in the reference's order from the whole record array
-(ffb_emit). The per-sum search cost grows about linearly with the sum (the cumulative cost of
-sums up to s grows as s^2), so shard boundaries are placed at equal shares of s^2.
+The prime map is split into equal byte slabs, one per rank (the reference likewise hands
+the map's slabs to its devices, source/pull_scheduler.cpp:149-202): each rank sieves its
+slab into its place in a full-size map buffer and an all-gather over NVLink fills in the
+other ranks' slabs, so every rank holds the whole map after sieving 1/N of it. The odd sums
+are independent, so they split into contiguous shards, one per rank, searched with no
+exchange; the packed records are gathered to rank 0, which emits ff_seg's text in the
+reference's order from the whole record array (ffb_emit). The per-sum search cost grows
+about linearly with the sum (the cumulative cost of sums up to s grows as s^2), so shard
+boundaries are placed at equal shares of s^2.
 """
 import math
 
@@ -28,6 +31,29 @@ def shard_bounds(lo, hi, world, rank):
     a = lo if rank == 0 else cut(rank / world)
     b = hi if rank == world - 1 else cut((rank + 1) / world) - 2
     return a, b
+
+
+def map_slab(mpv, world, rank):
+    """Rank's slab of the prime map for values 0..mpv: (seg_lo, seg_hi, slab_bytes). Every
+    slab is slab_bytes long (a multiple of 256 bytes, so each starts 16-byte aligned at a
+    value that is a multiple of 4096) and rank r's starts at byte r * slab_bytes of a buffer
+    of world * slab_bytes bytes; the values [seg_lo, seg_hi) are sieved into it (seg_hi <=
+    seg_lo for a rank past the end of the map: nothing to sieve)."""
+    map_bytes = (mpv + 1 + 15) >> 4
+    slab = -(-map_bytes // world)
+    slab = -(-slab // 256) * 256
+    lo = min(rank * slab * 16, mpv + 1)
+    hi = min((rank + 1) * slab * 16, mpv + 1)
+    return lo, hi, slab
+
+
+def gather_map(dist, full, slab_bytes):
+    """In-place all-gather of the ranks' map slabs: `full` (uint8, world * slab_bytes) holds
+    this rank's slab at its place; afterwards it holds every rank's."""
+    world = dist.get_world_size()
+    rank = dist.get_rank()
+    mine = full[rank * slab_bytes:(rank + 1) * slab_bytes]
+    dist.all_gather_into_tensor(full[:world * slab_bytes], mine)
 
 
 def gather_records(dist, local, lo, hi, world, rank):

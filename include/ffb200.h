@@ -226,8 +226,9 @@ uint64_t ffb_probe_bound(uint32_t maxSum);
  * which each GPU that loads the library holds until the process exits.
  *   - Same inputs and output as ffb_search_async: odd sums lo..hi (lo odd, hi <= 2^25; other
  *     ranges are rejected with -1 and a message), d_map/mapBound, d_rec zero-filled by the
- *     call. d_err (optional, device) receives the error flags of ffb_take_errors; NULL keeps
- *     them in the library's array.
+ *     call. d_err (required, one device word) is cleared by the call and receives the error
+ *     flags that ffb_take_errors would report; a NULL d_err is rejected with -1, since no
+ *     other call could read the flags back.
  *   - The first call on a device sets the array up (its device address, the prime table
  *     copied in, synchronously) with that device current; make that first call before any
  *     stream capture.
@@ -236,6 +237,21 @@ uint64_t ffb_probe_bound(uint32_t maxSum);
  *     on it: serialise them. */
 int ffb_search_noalloc(int deviceIndex, const uint8_t* d_map, uint64_t mapBound, uint32_t lo,
                        uint32_t hi, uint64_t* d_rec, uint32_t* d_err, void* stream);
+
+/* Measured on-chip peaks of the device (no reference counterpart): the denominators of the
+ * search's integer roofline and of the sieve's marking roofline. Each figure is operations
+ * per second over the whole GPU from a microbenchmark timed with CUDA events (about 0.1 s in
+ * all): 32-bit multiply-adds, 32-bit ALU operations, full 64x64->128-bit products, integer
+ * operations with multiply-adds and ALU operations mixed one to two, shared-memory atomicAnd
+ * with the 32 lanes of a warp on distinct banks and on pseudo-random words, and plain
+ * shared-memory read-modify-writes. */
+typedef struct {
+    double imad32PerS, alu32PerS, mul64PerS, intOpsPerS;
+    double atomsConflictFreePerS, atomsRandomPerS, smemRmwPerS;
+    int sms;
+    double clockMhz;
+} FfbPeaks;
+int ffb_measure_peaks(int deviceIndex, FfbPeaks* out);
 
 /* Reads and clears the device error flags raised by kernels (1: Miller-Rabin outside the
  * exact domain, 2: a divisor list overflowed, 4: bad launch input). Synchronises the
@@ -260,7 +276,8 @@ int ffb_context_set_map_budget(FfbContext* ctx, uint64_t bytes);
  * map is sieved for the whole batch, the sums of all ranges' schedules are merged into
  * disjoint intervals that one persistent search launch takes as its work queue (each shared
  * sum evaluated once), and both launches are captured once into a CUDA graph. autotune != 0
- * times the sieve tile sizes (64..216 KB) and search block sizes (4, 8, 16 warps) on the
+ * times the sieve tile sizes (64..216 KB), then the search's block size (4, 8, 16 warps)
+ * and sums per chunk (16, 32, 64 sums a warp takes from the work queue at a time) on the
  * batch first (kept per map size and sum count for later batches). Each range's text is
  * exactly what ff_seg prints for it; the timing lines carry the batch's sieve and search
  * times. Allocates its device buffers at creation. */
@@ -272,6 +289,7 @@ typedef struct {
     uint32_t sieveTileBytes, searchWarps;
     int autotuned;              /* 0 fixed defaults, 1 timed at creation, 2 reused */
     float sieveMs, searchMs;    /* device times of the last completed launch */
+    uint32_t searchChunk;       /* sums per chunk of the work queue */
 } FfbBatchInfo;
 FfbBatch* ffb_batch_create(int deviceIndex, uint32_t n, const int32_t* starts,
                            const int32_t* limits, int autotune);
@@ -380,6 +398,16 @@ int ffb_serve_info(FfbServer* s, FfbServeInfo* out);
 int ffb_serve_drain(FfbServer* s, int timeoutMs);
 /* Finishes the launches in flight, drops undelivered output and frees everything. */
 void ffb_serve_destroy(FfbServer* s);
+
+/* One slab of the prime map: the values [segLo, segHi) of ff_seg's map (every odd prime p
+ * with p*p < segHi marks; the value 1 is cleared when segLo == 0) written to d_out in the
+ * map's own layout, so d_out is the map's byte segLo/16 and (segHi-segLo+15)/16 bytes are
+ * written (bits of values >= segHi stay 1). segLo must be a multiple of 256 (d_out 16-byte
+ * aligned within the map). A sharded job sieves one slab per rank and all-gathers them; the
+ * reference distributes the map's slabs over its devices the same way
+ * (source/pull_scheduler.cpp:149-202). Asynchronous on `stream`. */
+int ffb_sieve_map_range_async(int deviceIndex, uint64_t segLo, uint64_t segHi, uint8_t* d_out,
+                              void* stream);
 
 /* The whole `ff_sieve` / ff_seg stdout for the given arguments (see ffb_geometry), with the
  * timing lines in microseconds ("Prime time: <us> μs", "Freudenthal time: <us> μs").

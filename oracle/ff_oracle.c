@@ -779,6 +779,49 @@ static int sb_put(sbuf* b, const char* s, size_t n)
     return 0;
 }
 
+/* The text ff_seg prints for one argument list, from per-sum records: the header, the
+ * solution lines of the schedule in emission order (segmentedSieve.C:763-791, 816-819) and
+ * the two timing lines normalised to "N". rec[(s - rec_lo)/2] = low<<32 | high or 0 for the
+ * odd sums rec_lo, rec_lo+2, ...; every sum of the schedule must be covered. */
+char* ffo_emit(const ffo_ctx* c, int nargs, int32_t a1, int32_t a2, const uint64_t* rec,
+               uint32_t rec_lo, uint64_t nrec, size_t* len)
+{
+    uint32_t ss, sl;
+    ffo_parse_args(nargs, a1, a2, &ss, &sl);
+    ffo_geometry g;
+    char hdr[2048];
+    int hn = ffo_geometry_headers(ss, sl, &g, hdr, sizeof hdr);
+    if (hn < 0 || g.too_big) return NULL;
+    int cap = 4 * (int)FFO_THREADS + 8;
+    uint32_t firsts[4 * FFO_THREADS + 8], lasts[4 * FFO_THREADS + 8];
+    int nr = ffo_schedule(ss, sl, g.max_prime_map_value, FFO_THREADS, firsts, lasts, cap);
+    if (nr < 0) return NULL;
+    const uint64_t rec_hi = (uint64_t)rec_lo + 2 * (nrec ? nrec - 1 : 0);
+    for (int r = 0; r < nr; ++r) {
+        uint32_t f = firsts[r] | 1u;
+        if (f > lasts[r]) continue;
+        uint32_t l = lasts[r] - !(lasts[r] & 1);
+        if (!rec || nrec == 0 || !(rec_lo & 1) || f < rec_lo || l > rec_hi) return NULL;
+    }
+    sbuf out = {0};
+    sb_put(&out, hdr, (size_t)hn);
+    uint32_t count = 0;
+    char line[256];
+    for (int r = 0; r < nr; ++r) {
+        for (uint32_t s = firsts[r] | 1u; s <= lasts[r]; s += 2) {
+            uint64_t v = rec[(s - rec_lo) / 2];
+            if (!v) continue;
+            int n = ffo_format_line(c, ++count, s, (uint32_t)(v >> 32), (uint32_t)v, line,
+                                    sizeof line);
+            sb_put(&out, line, (size_t)n);
+        }
+    }
+    const char* tail = "Prime time: N \xce\xbcs\nFreudenthal time: N \xce\xbcs\n";
+    sb_put(&out, tail, strlen(tail));
+    if (len) *len = out.n;
+    return out.p;
+}
+
 char* ffo_run(int nargs, int32_t a1, int32_t a2, uint64_t map_bound, int nthreads, size_t* len,
               ffo_counters* k)
 {
@@ -802,29 +845,24 @@ char* ffo_run(int nargs, int32_t a1, int32_t a2, uint64_t map_bound, int nthread
     ffo_ctx* c = ffo_create(hi > sl ? hi : sl, map_bound ? map_bound : g.max_prime_map_value,
                             nthreads);
     if (!c) return NULL;
-    sbuf out = {0};
-    sb_put(&out, hdr, (size_t)hn);
     uint64_t* rec = NULL;
+    uint64_t nrec = 0;
     if (lo <= hi) {
         hi -= !(hi & 1);   /* last odd sum */
-        rec = calloc(((uint64_t)hi - lo) / 2 + 1, sizeof(uint64_t));
+        nrec = ((uint64_t)hi - lo) / 2 + 1;
+        rec = calloc(nrec, sizeof(uint64_t));
         ffo_eval_range(c, lo, hi, rec, nthreads, k);
+    } else {
+        lo = 1;
     }
-    uint32_t count = 0;
-    char line[256];
-    for (int r = 0; r < nr; ++r) {
-        for (uint32_t s = firsts[r] | 1u; s <= lasts[r]; s += 2) {
-            uint64_t v = rec[(s - lo) / 2];
-            if (!v) continue;
-            int n = ffo_format_line(c, ++count, s, (uint32_t)(v >> 32), (uint32_t)v, line,
-                                    sizeof line);
-            sb_put(&out, line, (size_t)n);
-        }
+    char* out = NULL;
+    if (nrec) {
+        out = ffo_emit(c, nargs, a1, a2, rec, lo, nrec, len);
+    } else {
+        uint64_t dummy = 0;   /* no sums in the schedule: header and timing lines only */
+        out = ffo_emit(c, nargs, a1, a2, &dummy, 1, 1, len);
     }
-    const char* tail = "Prime time: N \xce\xbcs\nFreudenthal time: N \xce\xbcs\n";
-    sb_put(&out, tail, strlen(tail));
     free(rec);
     ffo_destroy(c);
-    if (len) *len = out.n;
-    return out.p;
+    return out;
 }

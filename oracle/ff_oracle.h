@@ -130,6 +130,13 @@ char* ffo_run(int nargs, int32_t a1, int32_t a2, uint64_t map_bound, int nthread
               size_t* len, ffo_counters* k);
 void  ffo_free(void* p);
 
+/* The same text from per-sum records already evaluated (rec[(s - rec_lo)/2] for the odd sums
+ * rec_lo .. rec_lo + 2*(nrec-1), which must cover the schedule of the argument list), with c
+ * answering the prime tags of the terms. Lets many argument lists share one evaluation of
+ * the union of their sums. NULL when the records do not cover the schedule. */
+char* ffo_emit(const ffo_ctx* c, int nargs, int32_t a1, int32_t a2, const uint64_t* rec,
+               uint32_t rec_lo, uint64_t nrec, size_t* len);
+
 #ifdef __cplusplus
 }
 #endif

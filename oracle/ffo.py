@@ -70,6 +70,9 @@ def load():
                                           ctypes.c_uint64, ctypes.c_int,
                                           ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(Counters)]),
             "ffo_free": (None, [ctypes.c_void_p]),
+            "ffo_emit": (ctypes.c_void_p, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int32,
+                                           ctypes.c_int32, u64p, ctypes.c_uint32, ctypes.c_uint64,
+                                           ctypes.POINTER(ctypes.c_size_t)]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(lib, name)
@@ -147,6 +150,22 @@ class Context:
         if rc:
             raise ValueError("eval_range")
         return out, k.as_dict()
+
+    def emit(self, args, rec, rec_lo):
+        """ff_seg's stdout (timing lines as N) for the argument list from per-sum records
+        rec (numpy uint64, rec[(s - rec_lo)/2]) that cover its schedule."""
+        import numpy as np
+        rec = np.ascontiguousarray(rec, dtype=np.uint64)
+        a = list(args) + [0, 0]
+        n = ctypes.c_size_t()
+        p = self.lib.ffo_emit(self.h, len(args), a[0], a[1], rec.ctypes.data_as(u64p), rec_lo,
+                              len(rec), ctypes.byref(n))
+        if not p:
+            raise ValueError(f"records do not cover the schedule of {args}")
+        try:
+            return ctypes.string_at(p, n.value)
+        finally:
+            self.lib.ffo_free(p)
 
 
 def odd_primes(limit):

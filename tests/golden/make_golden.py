@@ -19,7 +19,8 @@ scripts/verify.sh does, and writes:
                          lists of `ff_seg --dump-map <file> ...`, the size and sha256 of the
                          dumped prime map and the stdout printed before the dump
 
-Needs the reference checkout; run from the repository root:
+Needs the reference checkout ($FF_REF_DIR, default ../reference beside the repository);
+run from the repository root:
     python tests/golden/make_golden.py [--dump-maps | --pen-blocks]
 """
 import hashlib
@@ -33,7 +34,8 @@ import tempfile
 
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "ff_seg")
-REF_TREE = "/root/reference"
+# the reference checkout: $FF_REF_DIR, by default a sibling of this repository
+REF_TREE = os.environ.get("FF_REF_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
 OUT = os.path.join(ROOT, "tests", "golden")
 NORM = re.compile(rb"(Prime|Freudenthal) time: [0-9]+")
 

@@ -85,6 +85,28 @@ def test_served_stream_identity_alone_vs_mix(ffb, oracle):
         assert norm(mix[k]) == norm(oracle.run(s, l, map_bound=(1 << 30) - 1)), (s, l)
 
 
+def test_served_stream_matches_oracle(ffb):
+    """The first 300 requests of the seed-1 served stream (limits up to 2^22, 154 of them
+    above 2^21) submitted as one burst under the 8 GiB budget (a map capped below the
+    probes, Miller-Rabin above it): every request's streamed text equals the oracle's
+    (tests/golden/served_seed1.json, made by tests/golden/make_workload_golden.py)."""
+    import json
+    import os
+    import workloads
+    with open(os.path.join(os.path.dirname(__file__), "golden", "served_seed1.json")) as f:
+        fix = json.load(f)["ranges"]
+    reqs = [(s, l) for _, s, l in workloads.served_requests(seed=1)[:len(fix)]]
+    assert [tuple(r["args"]) for r in fix] == reqs and len(fix) >= 300
+    assert sum(1 for _, l in reqs if l > 1 << 21) >= 100
+    with ffb.Server(budget_bytes=8 << 30) as srv:
+        ids = [srv.submit(s, l) for s, l in reqs]
+        texts = srv.collect(ids)
+        info = srv.info()
+    assert info["failed"] == 0 and info["mapMaxValue"] < ffb.load().ffb_probe_bound(1 << 22)
+    bad = [r["args"] for r, t in zip(fix, texts) if t is None or sha(t) != r["sha256"]]
+    assert not bad, bad
+
+
 def test_streamed_chunks_arrive_in_order(ffb):
     """A request sliced over many launches streams its chunks in order; the header leads."""
     with ffb.Server(budget_bytes=8 << 30, launch_work=2048) as srv:

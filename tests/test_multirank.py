@@ -99,6 +99,67 @@ def test_sharded_odd_range(tmp_path, oracle, ffb):
     assert norm(text) == norm(oracle.run(*args, map_bound=(1 << 32) - 1))
 
 
+def _slab_worker(rank, world, port, mpv, out_path):
+    for p in (PKG, ORACLE):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    import math
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import ffo
+    from shard import gather_map, map_slab
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        lo, hi, slab = map_slab(mpv, world, rank)
+        full = torch.full((world * slab,), 0xA5, dtype=torch.uint8)
+        if hi > lo:
+            # the rank's slab as the device's slab sieve writes it (the reference slab
+            # contract, source/sieve_slab_kernel.h:40-107, with the map's list)
+            primes = ffo.odd_primes(math.isqrt(mpv))
+            part = ffo.slab_relative(lo, hi, primes)[:(hi - lo + 15) >> 4]
+            full[rank * slab:rank * slab + part.size] = torch.from_numpy(part)
+        gather_map(dist, full, slab)
+        if rank == 0:
+            np.save(out_path, full.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,mpv", [(2, 10_000_015), (3, 10_000_015), (3, 4_015)])
+def test_map_slabs_all_gathered(world, mpv, tmp_path, oracle):
+    """Each rank sieves its slab of the map (map_slab) and the in-place all-gather
+    (gather_map) leaves the byte-exact map of values 0..mpv on every rank; slabs past the end
+    of a small map stay empty."""
+    import multiprocessing as mp
+    import numpy as np
+    sys.path.insert(0, PKG)
+    from shard import map_slab
+    ctx = mp.get_context("spawn")
+    port = _free_port()
+    out = str(tmp_path / "map.npy")
+    procs = [ctx.Process(target=_slab_worker, args=(r, world, port, mpv, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=300)
+    codes = [p.exitcode for p in procs]
+    for p in procs:
+        if p.is_alive():
+            p.kill()
+    assert codes == [0] * world, codes
+    got = np.load(out)
+    want = oracle.build_map(mpv)
+    nbytes = (mpv + 1 + 15) >> 4
+    assert np.array_equal(got[:nbytes], want[:nbytes])
+    bounds = [map_slab(mpv, world, r) for r in range(world)]
+    assert bounds[0][0] == 0 and max(b[1] for b in bounds) == mpv + 1
+    assert all(b[0] % 4096 == 0 for b in bounds if b[1] > b[0])
+
+
 def test_shard_bounds_partition():
     sys.path.insert(0, PKG)
     from shard import odd_sums, shard_bounds
