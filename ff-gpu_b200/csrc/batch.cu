@@ -8,9 +8,10 @@
 //     to ONE persistent search launch as its work queue (largest sums first), each sum
 //     evaluated once however many ranges share it;
 //   * the sieve and the search launches captured once into a CUDA graph and replayed;
-//   * the sieve's tile size, the search's block size (warps per block) and the sums a warp
-//     takes per pull of the work queue (sums per chunk; sums per block = warps x chunk)
-//     picked by a small autotuner that times the candidates on the batch itself.
+//   * the sieve's tile size, the search's block size (warps per block), the warps that share
+//     one sum (1, 2 or 4) and the sums taken per pull of the work queue (sums per chunk;
+//     sums per block = warps x chunk / warps per sum) picked by a small autotuner that times
+//     the candidates on the batch itself.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -42,7 +43,7 @@ struct Interval {
 };
 
 struct Tuned {
-    uint32_t tile_bytes, warps, chunk;
+    uint32_t tile_bytes, warps, chunk, group;
 };
 std::mutex g_tune_mu;
 std::map<std::pair<uint64_t, uint64_t>, Tuned> g_tuned;  // (map bytes, sums) -> choice
@@ -60,7 +61,7 @@ struct FfbBatch {
     std::vector<uint64_t> rec_base;  // per interval (ascending order)
     uint64_t nrec = 0;
     uint64_t map_mpv = 0, map_bytes = 0;
-    uint32_t tile_bytes = 0, warps = 8, chunk = 32;
+    uint32_t tile_bytes = 0, warps = 8, chunk = 32, group = 1;
     int tuned = 0;
     // device
     uint8_t* d_map = nullptr;
@@ -115,6 +116,7 @@ SearchArgs search_args(const FfbBatch* b, const DeviceState* s)
     a.nchunks = b->nchunks;
     a.warps = b->warps;
     a.chunk = b->chunk;
+    a.group = b->group;
     return a;
 }
 
@@ -171,6 +173,7 @@ int autotune(FfbBatch* b)
             b->tile_bytes = it->second.tile_bytes;
             b->warps = it->second.warps;
             b->chunk = it->second.chunk;
+            b->group = it->second.group;
             b->tuned = 2;
             return build_queue(b) || build_sieve(b);
         }
@@ -197,10 +200,14 @@ int autotune(FfbBatch* b)
     if (enqueue_sieve_plan(b->sieve, b->stream)) return -1;  // the map the search reads
     DeviceState* s = device_state(b->dev);
     if (!s) return -1;
+    // (warps per sum, sums per chunk): one warp per sum with 16, 32 or 64 sums per pull, or
+    // 2 / 4 warps per sum with 32 sums per warp of the group; each with 4, 8, 16 warps a block
+    const uint32_t shapes[][2] = {{1, 16}, {1, 32}, {1, 64}, {2, 64}, {4, 128}};
     best = 1e30f;
-    uint32_t best_w = 8, best_c = 32;
-    for (uint32_t c : {16u, 32u, 64u}) {
-        b->chunk = c;
+    uint32_t best_w = 8, best_c = 32, best_g = 1;
+    for (const auto& sh : shapes) {
+        b->group = sh[0];
+        b->chunk = sh[1];
         if (build_queue(b)) return -1;
         for (uint32_t w : {4u, 8u, 16u}) {
             b->warps = w;
@@ -210,15 +217,16 @@ int autotune(FfbBatch* b)
             FFB_CUDA(cudaEventRecord(b->ev[2], b->stream));
             FFB_CUDA(cudaStreamSynchronize(b->stream));
             const float ms = elapsed(b->ev[1], b->ev[2]);
-            if (ms < best) { best = ms; best_w = w; best_c = c; }
+            if (ms < best) { best = ms; best_w = w; best_c = b->chunk; best_g = b->group; }
         }
     }
     b->warps = best_w;
     b->chunk = best_c;
+    b->group = best_g;
     if (build_queue(b)) return -1;
     b->tuned = 1;
     std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tuned[key] = {b->tile_bytes, b->warps, b->chunk};
+    g_tuned[key] = {b->tile_bytes, b->warps, b->chunk, b->group};
     return 0;
 }
 
@@ -433,6 +441,7 @@ extern "C" int ffb_batch_info(const FfbBatch* b, FfbBatchInfo* info)
     info->sieveTileBytes = b->tile_bytes;
     info->searchWarps = b->warps;
     info->searchChunk = b->chunk;
+    info->searchGroup = b->group;
     info->autotuned = b->tuned;
     info->sieveMs = 0;
     info->searchMs = 0;

@@ -96,7 +96,7 @@ static unsigned long long* stats_words(DeviceState* s)
 // Search over odd sums lo..hi into packed records and/or GpuRecord slots.
 int run_search(int dev, const uint8_t* d_map, uint64_t bound, uint32_t lo, uint32_t hi,
                uint64_t* d_rec, void* grec, uint32_t grec_base, uint32_t* gcount,
-               cudaStream_t stream)
+               cudaStream_t stream, uint32_t warps, uint32_t chunk, uint32_t group)
 {
     if (!(lo & 1) || hi < lo || hi >= (1u << 25) + 1 || !d_map) {
         std::fprintf(stderr, "ffb: search range [%u, %u] not supported (odd sums up to 2^25)\n",
@@ -122,6 +122,9 @@ int run_search(int dev, const uint8_t* d_map, uint64_t bound, uint32_t lo, uint3
     a.sched = sched_slot(s);
     a.err = err_word(s);
     a.stats = stats_words(s);
+    a.warps = warps;
+    a.chunk = chunk;
+    a.group = group;
     if (d_rec) FFB_CUDA(cudaMemsetAsync(d_rec, 0, 8ull * a.nsums, stream));
     FFB_CUDA(cudaMemsetAsync(a.sched, 0, 4, stream));
     return launch_search(a, s->sms, stream);
@@ -500,6 +503,19 @@ extern "C" int ffb_search_async(int deviceIndex, const uint8_t* d_map, uint64_t 
 {
     return run_search(deviceIndex, d_map, mapBound, lo, hi, d_rec, nullptr, 0, nullptr,
                       (cudaStream_t)stream);
+}
+
+extern "C" int ffb_search_shape_async(int deviceIndex, const uint8_t* d_map, uint64_t mapBound,
+                                      uint32_t lo, uint32_t hi, uint64_t* d_rec, uint32_t warps,
+                                      uint32_t chunk, uint32_t group, void* stream)
+{
+    if ((warps != 4 && warps != 8 && warps != 16) || (group != 1 && group != 2 && group != 4)) {
+        std::fprintf(stderr, "ffb_search_shape_async: %u warps per block, %u per sum not offered\n",
+                     warps, group);
+        return -1;
+    }
+    return run_search(deviceIndex, d_map, mapBound, lo, hi, d_rec, nullptr, 0, nullptr,
+                      (cudaStream_t)stream, warps, chunk, group);
 }
 
 extern "C" int ffb_search_stats(int deviceIndex, uint64_t* out, int reset)

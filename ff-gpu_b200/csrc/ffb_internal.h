@@ -35,6 +35,8 @@ struct SearchArgs {
     uint32_t nchunks = 0;   // chunks of `chunk` sums over all intervals
     uint32_t warps = 0;     // warps per block: 4, 8 or 16 (0: 16 map-only, 8 Miller-Rabin)
     uint32_t chunk = 32;    // sums a warp takes per pull of the work counter: 16, 32 or 64
+                            // (one warp per sum), 32 * group with group > 1
+    uint32_t group = 1;     // warps per sum: 1, or 2 / 4 (map-only variant)
 };
 
 // Packed per-sum record written by the search: 0 = no solution line, else
@@ -90,7 +92,7 @@ int run_sieve_map(int dev, uint64_t seg_lo, uint64_t seg_hi, uint8_t* d_out, cud
 uint32_t* device_err_word(DeviceState* s);
 int run_search(int dev, const uint8_t* d_map, uint64_t bound, uint32_t lo, uint32_t hi,
                uint64_t* d_rec, void* grec, uint32_t grec_base, uint32_t* gcount,
-               cudaStream_t stream);
+               cudaStream_t stream, uint32_t warps = 0, uint32_t chunk = 32, uint32_t group = 1);
 
 // Odd primes <= limit into the host vector (ascending).
 void host_odd_primes(uint64_t limit, uint32_t** out, uint32_t* n);

@@ -322,6 +322,11 @@ struct SumState {
     uint32_t count;       // valid splits seen so far (saturating use: >= 2 means rejected)
     uint32_t ta, tb;      // terms of the first valid split
     uint32_t na, nb, nc;  // queue sizes
+    // several warps on one sum (search_kernel_group): the group's shared count of valid
+    // splits and the terms of the first, and this warp's share of the splits (part of parts)
+    uint32_t* gcount = nullptr;
+    uint32_t* gterms = nullptr;
+    uint32_t part = 0, parts = 1;
 };
 
 // Runs stage 1 on up to 32 queued items: passes go to queue b; with the Miller-Rabin variant,
@@ -423,7 +428,24 @@ __device__ void drain_b(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int la
         valid = act && stage2<kMR>(item, st.s, A, &a, &b);
     }
     const uint32_t m = __ballot_sync(0xFFFFFFFFu, valid);
-    if (m) {
+    if (st.gcount) {
+        // the group's count: add this drain's valid splits (the first one found anywhere in
+        // the group keeps its terms) and read what the other warps found
+        const int src = m ? __ffs(m) - 1 : 0;
+        a = __shfl_sync(0xFFFFFFFFu, a, src);
+        b = __shfl_sync(0xFFFFFFFFu, b, src);
+        uint32_t total = 0;
+        if (lane == 0) {
+            if (m) {
+                const uint32_t old = atomicAdd(st.gcount, (uint32_t)__popc(m));
+                if (old == 0) { st.gterms[0] = a; st.gterms[1] = b; }
+                total = old + __popc(m);
+            } else {
+                total = *(volatile uint32_t*)st.gcount;
+            }
+        }
+        st.count = __shfl_sync(0xFFFFFFFFu, total, 0);
+    } else if (m) {
         const int src = __ffs(m) - 1;
         a = __shfl_sync(0xFFFFFFFFu, a, src);
         b = __shfl_sync(0xFFFFFFFFu, b, src);
@@ -499,7 +521,7 @@ __device__ bool run_phase(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int 
         // odd o in [o0, omax] with o<<k <= s-3
         const uint32_t omax = (s - 3) >> k;
         const uint32_t n = omax >= o0 ? ((omax - o0) >> 1) + 1 : 0;
-        for (uint32_t base = 0; base < n; base += 64) {
+        for (uint32_t base = 64 * st.part; base < n; base += 64 * st.parts) {
             const uint32_t i0 = base + lane, i1 = i0 + 32;
             const uint32_t oa = o0 + 2 * i0, ob = o0 + 2 * i1;
             const int ca = stage0<kOdd, kMR>(s, k, oa, i0 < n, A);
@@ -659,7 +681,164 @@ __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
     }
 }
 
+// Several warps on one sum (map-only variant): a group of G warps takes chunks of 32*G sums;
+// each warp runs the lane-parallel filter on 32 of them and appends its survivors to the
+// group's list, then the G warps take the survivors one at a time, each enumerating every
+// G-th block of 64 splits (and every G-th Power2Composite item) with its own queues, adding
+// the valid splits it finds to the group's shared count. The verdict depends only on whether
+// exactly one split is valid, so how the splits are shared out does not change it. Warps of
+// a group meet at a named barrier (id 1 + group index) around each survivor.
+template <int G>
+struct GroupShared {
+    uint32_t chunk, n, count;
+    uint32_t terms[2];
+    uint32_t s[32 * G], ri[32 * G], cnt[32 * G], ta[32 * G], tb[32 * G], comp[32 * G];
+};
+
+__device__ __forceinline__ void group_bar(uint32_t id, uint32_t threads)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
+template <int W, int G>
+__global__ void __launch_bounds__(W * 32) search_kernel_group(const SearchArgs A)
+{
+    static_assert(G > 1 && W % G == 0 && W / G <= 15, "group shape");
+    __shared__ WarpQ<false> queues[W];
+    __shared__ GroupShared<G> groups[W / G];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t gi = warp / G, part = warp % G, bar = gi + 1, nthr = 32 * G;
+    WarpQ<false>& Q = queues[warp];
+    GroupShared<G>& gs = groups[gi];
+    const uint32_t K = 32 * G;  // sums per chunk
+    const uint32_t nchunks = A.nseg ? A.nchunks : (A.nsums + K - 1) / K;
+    if (part == 0 && lane == 0) gs.n = 0;
+    for (;;) {
+        if (part == 0 && lane == 0) gs.chunk = atomicAdd(A.sched, 1u);
+        group_bar(bar, nthr);
+        const uint32_t c = gs.chunk;
+        if (c >= nchunks) break;
+        // ---- lane-parallel: filter + Power2Prime for this warp's 32 sums of the chunk ----
+        bool act;
+        uint32_t s = 5, ri = 0;
+        if (A.nseg == 0) {
+            const uint32_t idx = c * K + 32 * part + lane;
+            act = idx < A.nsums;
+            if (act) {
+                s = A.hi - 2 * idx;
+                ri = (s - A.lo) >> 1;
+            }
+        } else {
+            uint32_t a = 0, b = A.nseg - 1;
+            while (a < b) {
+                const uint32_t m = (a + b + 1) >> 1;
+                if (__ldg(&A.seg[m].w) <= c) a = m; else b = m - 1;
+            }
+            const uint4 g = __ldg(&A.seg[a]);
+            const uint32_t idx = (c - g.w) * K + 32 * part + lane;
+            act = idx < g.y;
+            if (act) {
+                s = g.x + 2 * (g.y - 1 - idx);  // descending within the interval
+                ri = g.z + ((s - g.x) >> 1);
+            }
+        }
+        bool surv = false;
+        uint32_t cnt = 0, ta = 0, tb = 0, comp = 0;
+        if (act) {
+            // Sammy's first statement (reference/segmentedSieve.C:805-806)
+            const uint32_t d3 = s / 3;
+            const bool pass = !pair1<false>(A, s) && (s != 3 * d3 || isp<false>(A, d3));
+            if (pass) {
+                // Power2Prime (reference/segmentedSieve.C:547-564)
+                for (uint32_t even = 4, k = 2; even < s - 2; even <<= 1, ++k) {
+                    const uint32_t odd = s - even;
+                    if (isp<false>(A, odd)) {
+                        if (++cnt > 1) break;
+                        if (cnt == 1) { ta = even; tb = odd; }
+                    } else {
+                        comp |= 1u << k;
+                    }
+                }
+                surv = cnt <= 1;
+            }
+        }
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, surv);
+        uint32_t base = 0;
+        if (lane == 0 && m) base = atomicAdd(&gs.n, (uint32_t)__popc(m));
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (surv) {
+            const uint32_t j = base + __popc(m & ((1u << lane) - 1));
+            gs.s[j] = s;
+            gs.ri[j] = ri;
+            gs.cnt[j] = cnt;
+            gs.ta[j] = ta;
+            gs.tb[j] = tb;
+            gs.comp[j] = comp;
+        }
+        group_bar(bar, nthr);
+        // ---- the group on one survivor at a time ----
+        const uint32_t nsurv = gs.n;
+        for (uint32_t i = 0; i < nsurv; ++i) {
+            if (part == 0 && lane == 0) {
+                gs.count = gs.cnt[i];
+                gs.terms[0] = gs.ta[i];
+                gs.terms[1] = gs.tb[i];
+            }
+            group_bar(bar, nthr);
+            SumState st;
+            st.s = gs.s[i];
+            st.count = gs.cnt[i];
+            st.ta = st.tb = 0;
+            st.gcount = &gs.count;
+            st.gterms = gs.terms;
+            st.part = part;
+            st.parts = G;
+            st.na = 0;
+            st.nc = 0;
+            const uint32_t cmask = gs.comp[i];
+            // Power2Composite items (reference/segmentedSieve.C:591-605), every G-th to this warp
+            st.nb = push(Q.b, 0, ((cmask >> lane) & 1) && lane % G == part, enc(lane, 0, true), lane);
+            bool open = true;
+            if (st.nb >= 32) {
+                drain_b(st, Q, A, lane);
+                open = st.count <= 1;
+            }
+            if (open) open = run_phase<true, false>(st, Q, A, lane);
+            if (open) open = run_phase<false, false>(st, Q, A, lane);
+            while (open && st.na > 0) {
+                drain_a(st, Q, A, lane);
+                if (st.nb >= 32) { drain_b(st, Q, A, lane); open = st.count <= 1; }
+            }
+            while (open && st.nb > 0) {
+                drain_b(st, Q, A, lane);
+                open = st.count <= 1;
+            }
+            group_bar(bar, nthr);
+            if (part == 0 && lane == 0 && gs.count == 1)
+                write_result<false>(A, st.s, gs.ri[i], gs.terms[0], gs.terms[1]);
+            group_bar(bar, nthr);
+        }
+        if (part == 0 && lane == 0) gs.n = 0;
+    }
+}
+
 }  // namespace
+
+template <int W, int G>
+int launch_group(const SearchArgs& a, int sms, cudaStream_t stream)
+{
+    int per_sm = 0;
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel_group<W, G>, W * 32, 0));
+    if (per_sm < 1) per_sm = 1;
+    const uint32_t chunks = a.nseg ? a.nchunks : (a.nsums + 32 * G - 1) / (32 * G);
+    uint32_t blocks = (uint32_t)sms * (uint32_t)per_sm;
+    const uint32_t need = (chunks + W / G - 1) / (W / G);
+    if (blocks > need) blocks = need;
+    if (blocks == 0) return 0;
+    search_kernel_group<W, G><<<blocks, W * 32, 0, stream>>>(a);
+    FFB_CUDA(cudaGetLastError());
+    return 0;
+}
 
 template <int W, bool kMR>
 int launch_w(const SearchArgs& a, int sms, cudaStream_t stream)
@@ -682,12 +861,25 @@ int launch_w(const SearchArgs& a, int sms, cudaStream_t stream)
 int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
 {
     if (a.nseg == 0 && a.nsums == 0) return 0;
+    const uint64_t pb = ffb_probe_bound(a.hi);
+    const bool mr = pb == 0 || a.bound < pb;
+    if (a.group != 1) {
+        // several warps per sum: map-only variant, chunks of 32 sums per warp of the group
+        if ((a.group != 2 && a.group != 4) || a.chunk != 32 * a.group || mr) {
+            std::fprintf(stderr, "ffb: %u warps per sum needs chunks of %u sums and a map over "
+                         "every probe\n", a.group, 32 * a.group);
+            return -1;
+        }
+        switch (a.warps) {
+        case 4: return a.group == 2 ? launch_group<4, 2>(a, sms, stream) : launch_group<4, 4>(a, sms, stream);
+        case 8: return a.group == 2 ? launch_group<8, 2>(a, sms, stream) : launch_group<8, 4>(a, sms, stream);
+        default: return a.group == 2 ? launch_group<16, 2>(a, sms, stream) : launch_group<16, 4>(a, sms, stream);
+        }
+    }
     if (a.chunk != 16 && a.chunk != 32 && a.chunk != 64) {
         std::fprintf(stderr, "ffb: search chunk of %u sums (16, 32 or 64)\n", a.chunk);
         return -1;
     }
-    const uint64_t pb = ffb_probe_bound(a.hi);
-    const bool mr = pb == 0 || a.bound < pb;
     switch (a.warps) {
     case 4: return mr ? launch_w<4, true>(a, sms, stream) : launch_w<4, false>(a, sms, stream);
     case 8: return mr ? launch_w<8, true>(a, sms, stream) : launch_w<8, false>(a, sms, stream);

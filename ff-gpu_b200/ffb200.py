@@ -27,7 +27,7 @@ class FfbBatchInfo(ctypes.Structure):
                 ("mapBytes", ctypes.c_uint64), ("sieveTileBytes", ctypes.c_uint32),
                 ("searchWarps", ctypes.c_uint32), ("autotuned", ctypes.c_int),
                 ("sieveMs", ctypes.c_float), ("searchMs", ctypes.c_float),
-                ("searchChunk", ctypes.c_uint32)]
+                ("searchChunk", ctypes.c_uint32), ("searchGroup", ctypes.c_uint32)]
 
 
 class FfbGeometry(ctypes.Structure):
@@ -141,6 +141,10 @@ SIGNATURES = {
     "ffb_measure_peaks": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(FfbPeaks)]),
     "ffb_probe_bound": (ctypes.c_uint64, [ctypes.c_uint32]),
     "ffb_search_stats": (ctypes.c_int, [ctypes.c_int, u64p, ctypes.c_int]),
+    "ffb_search_shape_async": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
+                                              ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
+                                              ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32,
+                                              ctypes.c_void_p]),
     "ffb_search_noalloc": (ctypes.c_int, [ctypes.c_int, ctypes.c_void_p, ctypes.c_uint64,
                                           ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_void_p]),

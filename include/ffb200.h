@@ -206,6 +206,15 @@ int ffb_sieve_map_tiled_async(int deviceIndex, uint64_t maxPrimeMapValue, uint8_
 int ffb_search_async(int deviceIndex, const uint8_t* d_map, uint64_t mapBound, uint32_t lo,
                      uint32_t hi, uint64_t* d_rec, void* stream);
 
+/* ffb_search_async with an explicit launch shape (no reference counterpart): `warps` warps
+ * per block (4, 8, 16), `group` warps per sum (1; or 2, 4 when the map covers every probe,
+ * mapBound >= ffb_probe_bound(hi)) and `chunk` sums taken from the work counter at a time
+ * (16, 32, 64 with one warp per sum; 32 * group otherwise). These are the candidates the
+ * batch's autotuner times; every shape gives the same records. Other shapes return -1. */
+int ffb_search_shape_async(int deviceIndex, const uint8_t* d_map, uint64_t mapBound, uint32_t lo,
+                           uint32_t hi, uint64_t* d_rec, uint32_t warps, uint32_t chunk,
+                           uint32_t group, void* stream);
+
 /* Work done by the searches on a device since the last reset: out[0] = probes of
  * 2^k + o*b - 2 (one random map sector each), out[1] = AllButOne... evaluations.
  * Synchronises the device; reset != 0 clears the counters. */
@@ -276,9 +285,10 @@ int ffb_context_set_map_budget(FfbContext* ctx, uint64_t bytes);
  * map is sieved for the whole batch, the sums of all ranges' schedules are merged into
  * disjoint intervals that one persistent search launch takes as its work queue (each shared
  * sum evaluated once), and both launches are captured once into a CUDA graph. autotune != 0
- * times the sieve tile sizes (64..216 KB), then the search's block size (4, 8, 16 warps)
- * and sums per chunk (16, 32, 64 sums a warp takes from the work queue at a time) on the
- * batch first (kept per map size and sum count for later batches). Each range's text is
+ * times the sieve tile sizes (64..216 KB), then the search's block size (4, 8, 16 warps),
+ * warps per sum (1, 2, 4) and sums per chunk (16, 32, 64 sums a warp takes from the work
+ * queue at a time with one warp per sum; 32 per warp of a group) on the batch first (kept
+ * per map size and sum count for later batches). Each range's text is
  * exactly what ff_seg prints for it; the timing lines carry the batch's sieve and search
  * times. Allocates its device buffers at creation. */
 typedef struct FfbBatch FfbBatch;
@@ -290,6 +300,7 @@ typedef struct {
     int autotuned;              /* 0 fixed defaults, 1 timed at creation, 2 reused */
     float sieveMs, searchMs;    /* device times of the last completed launch */
     uint32_t searchChunk;       /* sums per chunk of the work queue */
+    uint32_t searchGroup;       /* warps per sum (1, 2 or 4) */
 } FfbBatchInfo;
 FfbBatch* ffb_batch_create(int deviceIndex, uint32_t n, const int32_t* starts,
                            const int32_t* limits, int autotune);

@@ -18,10 +18,12 @@ scripts/verify.sh does, and writes:
   dump_maps.json         with --dump-maps (only this file is written then): for argument
                          lists of `ff_seg --dump-map <file> ...`, the size and sha256 of the
                          dumped prime map and the stdout printed before the dump
+  above_2_21.json        with --above-2-21 (only this file is written then): stdout of ff_seg
+                         for short ranges with limits between 2.2M and 3.2M (above the legs)
 
 Needs the reference checkout ($FF_REF_DIR, default ../reference beside the repository);
 run from the repository root:
-    python tests/golden/make_golden.py [--dump-maps | --pen-blocks]
+    python tests/golden/make_golden.py [--dump-maps | --pen-blocks | --above-2-21]
 """
 import hashlib
 import json
@@ -140,9 +142,28 @@ def pen_blocks():
     print(f"wrote pen_blocks.json for {len(out)} legs")
 
 
+def above_2_21():
+    """ff_seg on short ranges whose limits lie above 2^21 (the served configuration's limits
+    reach 2^22): each run sieves the reference's own map, limit^2/256 bytes (19 to 40 GB
+    here), so the limits stop where this machine's memory does."""
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    cases = [[2200001, 2201000], [2500001, 2500300], [2750001, 2750150], [2999999, 3000100],
+             [3100001, 3100063], [3199901, 3200000]]
+    out = []
+    for c in cases:
+        text = ff_seg(*c)
+        out.append({"args": c, "sha256": hashlib.sha256(text).hexdigest(), "text": text.decode()})
+        print(f"ff_seg {c}: {text.count(b') sum =')} solutions", flush=True)
+    with open(os.path.join(OUT, "above_2_21.json"), "w") as f:
+        json.dump(out, f, indent=0)
+    print(f"wrote {len(out)} ranges to above_2_21.json")
+
+
 if __name__ == "__main__":
     import sys
-    if "--dump-maps" in sys.argv:
+    if "--above-2-21" in sys.argv:
+        above_2_21()
+    elif "--dump-maps" in sys.argv:
         dump_maps()
     elif "--pen-blocks" in sys.argv:
         pen_blocks()

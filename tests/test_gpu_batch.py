@@ -64,6 +64,7 @@ def test_batched_config_matches_oracle(ffb):
     assert info["autotuned"] in (1, 2)
     assert info["sieveTileBytes"] in {k * 1024 for k in (64, 96, 128, 160, 192, 216)}
     assert info["searchWarps"] in (4, 8, 16)
-    assert info["searchChunk"] in (16, 32, 64)
+    assert info["searchGroup"] in (1, 2, 4)
+    assert info["searchChunk"] in ((16, 32, 64) if info["searchGroup"] == 1 else (32 * info["searchGroup"],))
     assert info["sieveMs"] > 0 and info["searchMs"] > 0      # replayed graph timestamps
     assert ffb.take_errors(0) == 0

@@ -131,3 +131,39 @@ def test_run_with_a_capped_map(ffb, golden, args, budget):
     leg = golden["legs"][str(args[1])]
     assert hashlib.sha256(norm(text)).hexdigest() == leg["sha256"]
     assert ffb.take_errors() == 0
+
+
+def test_every_launch_shape_gives_the_same_records(ffb, oracle):
+    """ffb_search_shape_async over every shape the batch's autotuner times (warps per block,
+    warps per sum, sums per chunk): the records of a range near 2^19 all equal the ordinary
+    launch's, which equal the oracle's on the same sums; shapes outside the offered set and
+    several warps per sum over a map that does not cover every probe are refused."""
+    import torch
+    lib = ffb.load()
+    lo, hi = 450001, 524287
+    mpv = lib.ffb_probe_bound(hi)
+    d_map = torch.empty(((mpv + 1 + 15) >> 4) + 256, dtype=torch.uint8, device="cuda")
+    assert lib.ffb_sieve_map_async(0, mpv, d_map.data_ptr(), None) == 0
+    n = (hi - lo) // 2 + 1
+    want = torch.empty(n, dtype=torch.int64, device="cuda")
+    assert lib.ffb_search_async(0, d_map.data_ptr(), mpv, lo, hi, want.data_ptr(), None) == 0
+    torch.cuda.synchronize()
+    shapes = [(w, c, 1) for w in (4, 8, 16) for c in (16, 32, 64)] + \
+             [(w, 32 * g, g) for w in (4, 8, 16) for g in (2, 4)]
+    for w, c, g in shapes:
+        got = torch.full((n,), -1, dtype=torch.int64, device="cuda")
+        assert lib.ffb_search_shape_async(0, d_map.data_ptr(), mpv, lo, hi, got.data_ptr(), w, c, g,
+                                          None) == 0
+        torch.cuda.synchronize()
+        assert torch.equal(got, want), (w, c, g)
+    assert ffb.take_errors(0) == 0
+    # the oracle on the first 2000 sums (low<<32|high; the device adds the two prime flags)
+    with oracle.Context(hi + 2, map_bound=(1 << 32) - 1) as c:
+        rec, _ = c.eval_range(lo, lo + 3998)
+    w = want[:2000].cpu().numpy().view(np.uint64) & np.uint64(0x7FFFFFFF7FFFFFFF)
+    assert np.array_equal(w, rec)
+    p = d_map.data_ptr()
+    assert lib.ffb_search_shape_async(0, p, mpv, lo, hi, want.data_ptr(), 8, 48, 1, None) == -1
+    assert lib.ffb_search_shape_async(0, p, mpv, lo, hi, want.data_ptr(), 8, 32, 2, None) == -1
+    assert lib.ffb_search_shape_async(0, p, 1 << 20, lo, hi, want.data_ptr(), 8, 64, 2, None) == -1
+    assert lib.ffb_search_shape_async(0, p, mpv, lo, hi, want.data_ptr(), 12, 32, 1, None) == -1

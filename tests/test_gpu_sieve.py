@@ -148,3 +148,24 @@ def test_pool_ops_and_semantics(ffb, oracle):
     free = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_int, ctypes.c_void_p)(ops.free)
     p = alloc(0, 1 << 20)
     assert p and free(0, p) == 0
+
+
+@pytest.mark.parametrize("world", [2, 3, 8])
+def test_map_range_slabs_assemble_the_map(ffb, oracle, world):
+    """ffb_sieve_map_range_async on each rank's slab (shard.map_slab), written at its place in
+    one buffer, gives the whole map: what a sharded job all-gathers."""
+    import torch
+    from shard import map_slab
+    mpv = (1 << 28) + 12345 * 16 + 15
+    slab = map_slab(mpv, world, 0)[2]
+    d = torch.full((world * slab + 256,), 0xA5, dtype=torch.uint8, device="cuda")
+    lib = ffb.load()
+    for r in range(world):
+        lo, hi, _ = map_slab(mpv, world, r)
+        if hi > lo:
+            assert lib.ffb_sieve_map_range_async(0, lo, hi, d.data_ptr() + (lo >> 4), None) == 0
+    torch.cuda.synchronize()
+    n = (mpv + 1 + 15) >> 4
+    assert np.array_equal(d[:n].cpu().numpy(), oracle.build_map(mpv)[:n])
+    assert lib.ffb_sieve_map_range_async(0, 100, 1000, d.data_ptr(), None) == -1   # unaligned
+    assert ffb.take_errors(0) == 0
