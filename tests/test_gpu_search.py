@@ -167,3 +167,15 @@ def test_every_launch_shape_gives_the_same_records(ffb, oracle):
     assert lib.ffb_search_shape_async(0, p, mpv, lo, hi, want.data_ptr(), 8, 32, 2, None) == -1
     assert lib.ffb_search_shape_async(0, p, 1 << 20, lo, hi, want.data_ptr(), 8, 64, 2, None) == -1
     assert lib.ffb_search_shape_async(0, p, mpv, lo, hi, want.data_ptr(), 12, 32, 1, None) == -1
+    # below the probes (the Miller-Rabin variant) only one warp per sum and 32 sums a chunk
+    assert lib.ffb_search_shape_async(0, p, 1 << 20, lo, hi, want.data_ptr(), 8, 64, 1, None) == -1
+
+
+def test_ranges_above_2_21_match_reference_binary(ffb):
+    """ffb_run on the short ranges above 2^21 that the reference binary ran
+    (tests/golden/above_2_21.json)."""
+    import json
+    with open(os.path.join(ROOT, "tests", "golden", "above_2_21.json")) as f:
+        cases = json.load(f)
+    for c in cases:
+        assert sha(norm(ffb.run(*c["args"]))) == c["sha256"], c["args"]

@@ -122,3 +122,17 @@ def test_slab_relative_matches_literal_fill(oracle, lo, hi):
     got = oracle.slab_relative(lo, hi, primes)
     want = _segment_fill_py(lo, hi, primes, (hi + 15) >> 4)
     assert np.array_equal(got, want)
+
+
+def test_ranges_above_2_21_match_reference_binary(oracle):
+    """Short ranges with limits from 2.2M to 3.2M (the served configuration's limits reach
+    2^22, beyond the reference's legs), against the reference binary's output
+    (tests/golden/above_2_21.json): the oracle with a 2^30 map and Miller-Rabin above it."""
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "above_2_21.json")) as f:
+        cases = json.load(f)
+    assert len(cases) >= 5 and min(c["args"][1] for c in cases) > 1 << 21
+    for c in cases:
+        out = oracle.run(*c["args"], map_bound=(1 << 30) - 1)
+        assert sha(out) == c["sha256"], c["args"]
