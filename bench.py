@@ -161,11 +161,11 @@ def odd_primes_upto(n):
 
 def sieve_marks(mpv, tile_bytes):
     """Shared-memory marks sieve_tiles makes for the map of values 0..mpv: the comb primes
-    (41 <= p <= tile bits / 1024) mark every odd multiple from p^2, the larger primes the
-    multiples p*k, k >= p, with k prime to 30 (the patterns cover 3..37)."""
+    (83 <= p <= tile bits / 1024) mark every odd multiple from p^2, the larger primes the
+    multiples p*k, k >= p, with k prime to 30 (the patterns cover 3..79)."""
     import numpy as np
     p = odd_primes_upto(math.isqrt(mpv))
-    p = p[p >= 41]
+    p = p[p >= 83]
     pcomb = tile_bytes * 8 // 1024
     comb = p[p <= pcomb]
     wheel = p[p > pcomb]

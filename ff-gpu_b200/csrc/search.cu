@@ -16,10 +16,13 @@
 //     one split in eight) probes 2^k + o*b - 2, a random HBM sector; stage 2 (about one in
 //     a hundred) runs AllButOne... on the split's product.
 //   * AllButOne... is evaluated from the factorisations of o and b (both below the sum)
-//     instead of the reference's trial-division walk over all primes; the walk's divisor
-//     list, its partially-sorted skip (reference/segmentedSieve.C:451) and its early
-//     returns are replayed exactly from the factorisation, since every IsPrime it makes on
-//     the cofactor is a pure function of the factorisation.
+//     instead of the reference's trial-division walk over all primes: the pairs that walk
+//     tests are exactly those of the odd divisors up to the square-root limit and their
+//     2^k multiples, which an odometer over the exponents enumerates with no divisor list.
+//   * Launch shapes (the candidates the batch's autotuner times): 4, 8 or 16 warps a block;
+//     16, 32 or 64 sums per pull of the work counter (a compile-time parameter, so the
+//     one-warp-per-sum kernel carries no extra loop); or 2 or 4 warps sharing one sum
+//     (search_kernel_group), each enumerating every 2nd or 4th block of splits.
 #include "ffb200.h"
 #include "ffb_device.cuh"
 #include "ffb_internal.h"
@@ -28,14 +31,12 @@ namespace ffb {
 namespace {
 
 constexpr int kQueue = 64;       // per-warp queue capacity (entries)
-constexpr int kMaxPf = 12;       // distinct odd primes of a product < 2^48 (3*5*...*41 = 1.5e14)
-constexpr int kMaxDiv = 64;      // pending probes of one AllButOne... call (Miller-Rabin variant)
-constexpr uint32_t kPfMask = (1u << 26) - 1;
+constexpr int kMaxPf = 16;       // distinct odd prime factors of a product < 2^52
+constexpr int kMaxDiv = 64;      // divisor list of one AllButOne... call (Miller-Rabin variant)
 
-// Prime factorisation of an odd product: factor q (below 2^26) and exponent e packed as
-// q | e << 26, in the order found.
 struct Fac {
-    uint32_t pf[kMaxPf];
+    uint32_t q[kMaxPf];
+    uint32_t e[kMaxPf];
     int n;
 };
 
@@ -82,26 +83,15 @@ __device__ __forceinline__ int pair_class(const SearchArgs& A, uint64_t i)
     return above_map_class(n, A.err);
 }
 
-// Adds q^e to the factorisation (exponents of a prime met twice add up).
-__device__ __forceinline__ void fac_add(Fac& f, uint32_t q, uint32_t e, const SearchArgs& A)
-{
-    for (int j = 0; j < f.n; ++j)
-        if ((f.pf[j] & kPfMask) == q) {
-            f.pf[j] += e << 26;
-            return;
-        }
-    if (f.n < kMaxPf) f.pf[f.n++] = q | e << 26;
-    else atomicOr(A.err, kErrFactorList);
-}
-
-// The prime factors of an odd x < 2^26 added to f: trial division by the exact-division
-// table, the cofactor's primality read from the bitmap after every factor found.
+// Ascending prime factorisation of an odd x < 2^32 by the exact-division table, with the
+// cofactor's primality read from the bitmap after every factor found.
 template <bool kMR>
-__device__ void factor_into(uint32_t x, Fac& f, const SearchArgs& A)
+__device__ int factor_odd(uint32_t x, uint32_t* q, uint32_t* e, int cap, const SearchArgs& A)
 {
+    int cnt = 0;
     uint32_t n = x;
-    if (n <= 1) return;
-    if (isp<kMR>(A, n)) { fac_add(f, n, 1, A); return; }
+    if (n <= 1) return 0;
+    if (isp<kMR>(A, n)) { q[0] = n; e[0] = 1; return 1; }
     for (uint32_t i = 0; i < A.ntdiv; ++i) {
         const TDiv t = A.tdiv[i];
         if ((uint64_t)t.p * t.p > n) break;
@@ -109,12 +99,48 @@ __device__ void factor_into(uint32_t x, Fac& f, const SearchArgs& A)
         if (y <= t.lim) {
             uint32_t ex = 0;
             do { n = y; ++ex; y = n * t.inv; } while (y <= t.lim);
-            fac_add(f, t.p, ex, A);
-            if (n == 1) return;
-            if (isp<kMR>(A, n)) { fac_add(f, n, 1, A); return; }
+            if (cnt < cap) { q[cnt] = t.p; e[cnt] = ex; }
+            ++cnt;
+            if (n == 1) return cnt;
+            if (isp<kMR>(A, n)) {
+                if (cnt < cap) { q[cnt] = n; e[cnt] = 1; }
+                return cnt + 1;
+            }
         }
     }
-    if (n > 1) fac_add(f, n, 1, A);
+    if (n > 1) {
+        if (cnt < cap) { q[cnt] = n; e[cnt] = 1; }
+        ++cnt;
+    }
+    return cnt;
+}
+
+template <bool kMR>
+__device__ void factor_product(uint32_t a, uint32_t b, Fac& f, const SearchArgs& A)
+{
+    uint32_t qa[10], ea[10], qb[10], eb[10];
+    int na = factor_odd<kMR>(a, qa, ea, 10, A);
+    int nb = b == 1 ? 0 : factor_odd<kMR>(b, qb, eb, 10, A);
+    int i = 0, j = 0, n = 0;
+    while (i < na || j < nb) {
+        uint32_t q, e;
+        if (j >= nb || (i < na && qa[i] < qb[j])) { q = qa[i]; e = ea[i]; ++i; }
+        else if (i >= na || qb[j] < qa[i]) { q = qb[j]; e = eb[j]; ++j; }
+        else { q = qa[i]; e = ea[i] + eb[j]; ++i; ++j; }
+        if (n < kMaxPf) { f.q[n] = q; f.e[n] = e; }
+        ++n;
+    }
+    f.n = n < kMaxPf ? n : kMaxPf;
+}
+
+// x / d for an odd d that divides x: x times the inverse of d modulo 2^64 (Newton's
+// iteration from the seed (3d) xor 2, which is correct to 5 bits; four steps give 80).
+__device__ __forceinline__ uint64_t exact_quotient(uint64_t x, uint32_t d)
+{
+    uint64_t v = (3ull * d) ^ 2;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v *= 2 - (uint64_t)d * v;
+    return x * v;
 }
 
 // AllButOneProductOfTermPairsOfSumOfFactorPairsHasSingleFactorPair
@@ -128,7 +154,7 @@ __device__ void factor_into(uint32_t x, Fac& f, const SearchArgs& A)
 // with an odometer over the exponents (digit i counts the power of factor i, 5 bits each; a
 // digit that cannot grow without passing lim is reset and the next one grows), keeping per
 // digit the divisor made of the digits from i up; the cofactor oddProduct/d is an exact
-// double division (both below 2^53, the quotient an integer). No divisor list is stored.
+// division by d's inverse modulo 2^64. No divisor list is stored.
 template <bool kMR>
 __device__ __noinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const Fac& f,
                                          const SearchArgs& A)
@@ -138,66 +164,10 @@ __device__ __noinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const
     uint32_t nm = 0;
     if ((1ull << k) <= lim) nm += !pair1<kMR>(A, (1ull << k) + odd_product);
     const int n = f.n;
-    const double od = (double)odd_product;
-    uint32_t Sd[kMaxPf + 1];      // divisor of the digits i.. (at most lim < 2^26)
-    uint64_t ex = 0;              // digit values, 5 bits each
-    for (int j = 0; j <= n; ++j) Sd[j] = 1;
-    for (;;) {
-        int i = 0;
-        uint32_t q = 0;
-        for (; i < n; ++i) {
-            q = f.pf[i] & kPfMask;
-            const uint32_t e = f.pf[i] >> 26, a = (uint32_t)(ex >> (5 * i)) & 31;
-            if (a < e && (uint64_t)Sd[i] * q <= lim) break;
-            ex &= ~(31ull << (5 * i));
-            Sd[i] = Sd[i + 1];
-        }
-        if (i == n) break;
-        ex += 1ull << (5 * i);
-        const uint32_t d = Sd[i] * q;
-        for (int j = 0; j <= i; ++j) Sd[j] = d;
-        const uint64_t c = (uint64_t)__ddiv_rn(od, (double)d);   // odd_product / d, exact
-        if ((nm += !pair1<kMR>(A, d + (c << k))) > 1) return false;
-        if (((uint64_t)d << k) <= lim && (nm += !pair1<kMR>(A, ((uint64_t)d << k) + c)) > 1)
-            return false;
+    if (n > 12) {   // 12 digits of 5 bits fill the odometer; products < 2^48 have at most 12
+        atomicOr(A.err, kErrFactorList);
+        return false;
     }
-    return nm == 1;
-}
-
-// all_but_one for the Miller-Rabin variant: the same divisor pairs (same odometer), but a
-// pair sum whose probe lies above the map (and has no small factor) is appended to pend[]
-// instead of being tested here, so that the warp can test them 32 at a time. Returns the
-// count of pairs already known not to be single (2 once the verdict is "no"); the verdict is
-// "yes" iff that count plus the pending probes found composite is exactly 1 (the order of the
-// tests does not change it). *np receives the number of pending pair sums (at most kMaxDiv:
-// more raises kErrFactorList).
-__device__ __noinline__ uint32_t all_but_one_defer(uint32_t k, uint64_t odd_product, const Fac& f,
-                                                   const SearchArgs& A, uint64_t* pend,
-                                                   uint32_t* np)
-{
-    const uint64_t P = odd_product << k;
-    const uint64_t lim = isqrt64(P);
-    uint32_t nm = 0, nd = 0;
-    *np = 0;
-    // counts a pair sum: 0 not single, 1 single, 2 pending; returns true once the verdict is
-    // "no" (nm > 1) or the pending list is full
-    auto visit = [&](uint64_t v) {
-        const int c = pair_class(A, v);
-        if (c == 2) {
-            if (nd >= kMaxDiv) {
-                atomicOr(A.err, kErrFactorList);
-                nm = 2;
-                return true;
-            }
-            pend[nd++] = v;
-        } else {
-            nm += c == 0;
-        }
-        return nm > 1;
-    };
-    if ((1ull << k) <= lim && visit((1ull << k) + odd_product)) return 2;
-    const int n = f.n;
-    const double od = (double)odd_product;
     uint32_t Sd[kMaxPf + 1];
     uint64_t ex = 0;
     for (int j = 0; j <= n; ++j) Sd[j] = 1;
@@ -205,8 +175,8 @@ __device__ __noinline__ uint32_t all_but_one_defer(uint32_t k, uint64_t odd_prod
         int i = 0;
         uint32_t q = 0;
         for (; i < n; ++i) {
-            q = f.pf[i] & kPfMask;
-            const uint32_t e = f.pf[i] >> 26, a = (uint32_t)(ex >> (5 * i)) & 31;
+            q = f.q[i];
+            const uint32_t e = f.e[i], a = (uint32_t)(ex >> (5 * i)) & 31;
             if (a < e && (uint64_t)Sd[i] * q <= lim) break;
             ex &= ~(31ull << (5 * i));
             Sd[i] = Sd[i + 1];
@@ -215,9 +185,88 @@ __device__ __noinline__ uint32_t all_but_one_defer(uint32_t k, uint64_t odd_prod
         ex += 1ull << (5 * i);
         const uint32_t d = Sd[i] * q;
         for (int j = 0; j <= i; ++j) Sd[j] = d;
-        const uint64_t c = (uint64_t)__ddiv_rn(od, (double)d);   // odd_product / d, exact
-        if (visit(d + (c << k))) return 2;
-        if (((uint64_t)d << k) <= lim && visit(((uint64_t)d << k) + c)) return 2;
+        const uint64_t c = exact_quotient(odd_product, d);
+        if ((nm += !pair1<kMR>(A, d + (c << k))) > 1) return false;
+        if (((uint64_t)d << k) <= lim && (nm += !pair1<kMR>(A, ((uint64_t)d << k) + c)) > 1)
+            return false;
+    }
+    return nm == 1;
+}
+
+// all_but_one for the Miller-Rabin variant: the same divisor pairs in the same order, but a
+// pair sum whose probe lies above the map (and has no small factor) is appended to pend[]
+// instead of being tested here, so that the warp can test them 32 at a time. Returns the
+// count of pairs already known not to be single (2 once the verdict is "no"); the verdict is
+// "yes" iff that count plus the pending probes found composite is exactly 1 (the order of the
+// tests does not change it). *np receives the number of pending pair sums.
+__device__ __noinline__ uint32_t all_but_one_defer(uint32_t k, uint64_t odd_product, const Fac& f,
+                                                   const SearchArgs& A, uint64_t* pend,
+                                                   uint32_t* np)
+{
+    const uint64_t P = odd_product << k;
+    const uint64_t lim = isqrt64(P);
+    uint64_t F[kMaxDiv], C[kMaxDiv];
+    uint32_t nf = 0, npend = 0, nm = 0, nd = 0;
+    *np = 0;
+    // counts a pair sum: 0 not single, 1 single, 2 pending; returns true once nm > 1
+    auto visit = [&](uint64_t v) {
+        const int c = pair_class(A, v);
+        if (c == 2) pend[nd++] = v;
+        else nm += c == 0;
+        return nm > 1;
+    };
+    F[0] = 1ull << k;
+    C[0] = odd_product;
+    if (F[0] <= lim) {
+        visit(F[0] + C[0]);
+        nf = 1;
+    }
+    int idx = 0;
+    bool first = true;  // the reference tries 3 before its first IsPrime(testProduct)
+    for (;;) {
+        uint64_t q;
+        uint32_t e;
+        if (first) {
+            first = false;
+            if (f.n > 0 && f.q[0] == 3) { q = 3; e = f.e[0]; idx = 1; }
+            else continue;
+        } else {
+            if (idx >= f.n) break;                                   // testProduct == 1
+            q = f.q[idx];
+            e = f.e[idx];
+            if (idx == f.n - 1 && e == 1 && q > lim) break;          // prime cofactor > limit
+            ++idx;
+        }
+        const uint64_t qi = inv64(q);
+        uint64_t tf = q, tfi = qi;
+        for (uint32_t j = 0; j < e; ++j) {
+            if (tf <= lim) {
+                const uint64_t ctf = (odd_product * tfi) << k;     // P / tf, exact
+                if (visit(tf + ctf)) return 2;
+                if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return 2; }
+                F[nf + npend] = tf;
+                C[nf + npend] = ctf;
+                ++npend;
+                for (uint32_t g = 0; g < nf; ++g) {
+                    const uint64_t m = F[g] * tf;
+                    if (m <= lim) {
+                        const uint64_t cm = C[g] * tfi;              // C[g] / tf, exact
+                        if (visit(m + cm)) return 2;
+                        if (nf + npend >= kMaxDiv) { atomicOr(A.err, kErrFactorList); return 2; }
+                        F[nf + npend] = m;
+                        C[nf + npend] = cm;
+                        ++npend;
+                    } else {
+                        // skip the rest of this ascending run of F (reference :451)
+                        for (const uint64_t v = F[g]; g + 1 < nf && v <= F[g + 1]; ++g) {}
+                    }
+                }
+            }
+            tf *= q;
+            tfi *= qi;
+        }
+        nf += npend;
+        npend = 0;
     }
     *np = nd;
     return nm;
@@ -239,17 +288,14 @@ __device__ bool stage2(uint32_t item, uint32_t s, const SearchArgs& A, uint32_t*
     uint64_t odd_product;
     if (item & 32) {
         const uint32_t odd = s - (1u << k);
-        f.n = 0;
-        factor_into<kMR>(odd, f, A);
+        factor_product<kMR>(odd, 1, f, A);
         odd_product = odd;
         *ta = 1u << k;
         *tb = odd;
     } else {
         const uint32_t o = item >> 6;
         const uint32_t even = o << k, b = s - even;
-        f.n = 0;
-        factor_into<kMR>(o, f, A);
-        factor_into<kMR>(b, f, A);
+        factor_product<kMR>(o, b, f, A);
         odd_product = (uint64_t)o * b;
         *ta = even;
         *tb = b;
@@ -267,17 +313,14 @@ __device__ uint32_t stage2_defer(uint32_t item, uint32_t s, const SearchArgs& A,
     uint64_t odd_product;
     if (item & 32) {
         const uint32_t odd = s - (1u << k);
-        f.n = 0;
-        factor_into<true>(odd, f, A);
+        factor_product<true>(odd, 1, f, A);
         odd_product = odd;
         *ta = 1u << k;
         *tb = odd;
     } else {
         const uint32_t o = item >> 6;
         const uint32_t even = o << k, b = s - even;
-        f.n = 0;
-        factor_into<true>(o, f, A);
-        factor_into<true>(b, f, A);
+        factor_product<true>(o, b, f, A);
         odd_product = (uint64_t)o * b;
         *ta = even;
         *tb = b;
@@ -322,11 +365,14 @@ struct SumState {
     uint32_t count;       // valid splits seen so far (saturating use: >= 2 means rejected)
     uint32_t ta, tb;      // terms of the first valid split
     uint32_t na, nb, nc;  // queue sizes
-    // several warps on one sum (search_kernel_group): the group's shared count of valid
-    // splits and the terms of the first, and this warp's share of the splits (part of parts)
-    uint32_t* gcount = nullptr;
-    uint32_t* gterms = nullptr;
-    uint32_t part = 0, parts = 1;
+};
+
+// Several warps on one sum (search_kernel_group): the group's shared count of valid splits,
+// the terms of the first one found, and which share of the splits this warp takes.
+struct GroupRef {
+    uint32_t* count;
+    uint32_t* terms;
+    uint32_t part;
 };
 
 // Runs stage 1 on up to 32 queued items: passes go to queue b; with the Miller-Rabin variant,
@@ -377,9 +423,11 @@ __device__ void drain_c(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int la
     st.nb = push(Q.b, st.nb, prime && !from0, item, lane);
 }
 
-// Runs stage 2 on up to 32 queued items and adds the valid ones to the count.
-template <bool kMR>
-__device__ void drain_b(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int lane)
+// Runs stage 2 on up to 32 queued items and adds the valid ones to the count (with G > 1
+// warps on the sum, to the group's count, reading back what the other warps found).
+template <bool kMR, int G = 1>
+__device__ void drain_b(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int lane,
+                        const GroupRef* grp = nullptr)
 {
     const uint32_t take = st.nb < 32 ? st.nb : 32;
     const uint32_t base = st.nb - take;
@@ -428,20 +476,18 @@ __device__ void drain_b(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int la
         valid = act && stage2<kMR>(item, st.s, A, &a, &b);
     }
     const uint32_t m = __ballot_sync(0xFFFFFFFFu, valid);
-    if (st.gcount) {
-        // the group's count: add this drain's valid splits (the first one found anywhere in
-        // the group keeps its terms) and read what the other warps found
+    if constexpr (G > 1) {
         const int src = m ? __ffs(m) - 1 : 0;
         a = __shfl_sync(0xFFFFFFFFu, a, src);
         b = __shfl_sync(0xFFFFFFFFu, b, src);
         uint32_t total = 0;
         if (lane == 0) {
             if (m) {
-                const uint32_t old = atomicAdd(st.gcount, (uint32_t)__popc(m));
-                if (old == 0) { st.gterms[0] = a; st.gterms[1] = b; }
+                const uint32_t old = atomicAdd(grp->count, (uint32_t)__popc(m));
+                if (old == 0) { grp->terms[0] = a; grp->terms[1] = b; }
                 total = old + __popc(m);
             } else {
-                total = *(volatile uint32_t*)st.gcount;
+                total = *(volatile uint32_t*)grp->count;
             }
         }
         st.count = __shfl_sync(0xFFFFFFFFu, total, 0);
@@ -512,8 +558,9 @@ __device__ __forceinline__ int stage0(uint32_t s, uint32_t k, uint32_t o, bool a
 // Enumerates the splits of one phase for sum s: k = kfirst, kfirst+2, ... while o0<<k < s-2;
 // for each k the odd parts o = o0, o0+2, ... with o<<k < s-2, two per lane per step. Returns
 // false once the sum is rejected (two valid splits).
-template <bool kOdd, bool kMR>
-__device__ bool run_phase(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int lane)
+template <bool kOdd, bool kMR, int G = 1>
+__device__ bool run_phase(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int lane,
+                          const GroupRef* grp = nullptr)
 {
     const uint32_t s = st.s;
     const uint32_t o0 = kOdd ? 5 : 3;
@@ -521,7 +568,9 @@ __device__ bool run_phase(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int 
         // odd o in [o0, omax] with o<<k <= s-3
         const uint32_t omax = (s - 3) >> k;
         const uint32_t n = omax >= o0 ? ((omax - o0) >> 1) + 1 : 0;
-        for (uint32_t base = 64 * st.part; base < n; base += 64 * st.parts) {
+        uint32_t first = 0;
+        if constexpr (G > 1) first = 64 * grp->part;
+        for (uint32_t base = first; base < n; base += 64 * G) {
             const uint32_t i0 = base + lane, i1 = i0 + 32;
             const uint32_t oa = o0 + 2 * i0, ob = o0 + 2 * i1;
             const int ca = stage0<kOdd, kMR>(s, k, oa, i0 < n, A);
@@ -539,7 +588,7 @@ __device__ bool run_phase(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int 
                 } else if (st.na >= 32) {
                     drain_a(st, Q, A, lane);
                     if (st.nb >= 32) {
-                        drain_b(st, Q, A, lane);
+                        drain_b<kMR, G>(st, Q, A, lane, grp);
                         if (st.count > 1) return false;
                     }
                 }
@@ -570,13 +619,13 @@ __device__ void write_result(const SearchArgs& A, uint32_t s, uint32_t ri, uint3
     }
 }
 
-template <int W, bool kMR>
+template <int W, bool kMR, int K>
 __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
 {
+    static_assert(K == 16 || K == 32 || K == 64, "sums per chunk");
     __shared__ WarpQ<kMR> queues[W];
     const int lane = threadIdx.x & 31;
     WarpQ<kMR>& Q = queues[threadIdx.x >> 5];
-    const uint32_t K = A.chunk;     // sums per chunk: 16, 32 or 64
     const uint32_t nchunks = A.nseg ? A.nchunks : (A.nsums + K - 1) / K;
     for (;;) {
         uint32_t c = 0;
@@ -594,9 +643,10 @@ __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
             }
             g = __ldg(&A.seg[a]);
         }
+#pragma unroll 1
         for (uint32_t h = 0; h < K; h += 32) {
             // ---- lane-parallel: filter + Power2Prime for up to 32 sums (largest first) ----
-            bool act = h + lane < K;
+            bool act = K >= 32 || (uint32_t)lane < K;
             uint32_t s = 5, ri = 0;
             if (A.nseg == 0) {
                 const uint32_t idx = c * K + h + lane;
@@ -677,9 +727,10 @@ __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
                 if (open && st.count == 1 && lane == 0) write_result<kMR>(A, st.s, sri, st.ta, st.tb);
                 __syncwarp();
             }
-        }   // rounds of the chunk
+        }   // rounds of 32 sums of the chunk
     }
 }
+
 
 // Several warps on one sum (map-only variant): a group of G warps takes chunks of 32*G sums;
 // each warp runs the lane-parallel filter on 32 of them and appends its survivors to the
@@ -710,6 +761,7 @@ __global__ void __launch_bounds__(W * 32) search_kernel_group(const SearchArgs A
     const uint32_t gi = warp / G, part = warp % G, bar = gi + 1, nthr = 32 * G;
     WarpQ<false>& Q = queues[warp];
     GroupShared<G>& gs = groups[gi];
+    const GroupRef grp{&gs.count, gs.terms, part};
     const uint32_t K = 32 * G;  // sums per chunk
     const uint32_t nchunks = A.nseg ? A.nchunks : (A.nsums + K - 1) / K;
     if (part == 0 && lane == 0) gs.n = 0;
@@ -789,10 +841,6 @@ __global__ void __launch_bounds__(W * 32) search_kernel_group(const SearchArgs A
             st.s = gs.s[i];
             st.count = gs.cnt[i];
             st.ta = st.tb = 0;
-            st.gcount = &gs.count;
-            st.gterms = gs.terms;
-            st.part = part;
-            st.parts = G;
             st.na = 0;
             st.nc = 0;
             const uint32_t cmask = gs.comp[i];
@@ -800,17 +848,17 @@ __global__ void __launch_bounds__(W * 32) search_kernel_group(const SearchArgs A
             st.nb = push(Q.b, 0, ((cmask >> lane) & 1) && lane % G == part, enc(lane, 0, true), lane);
             bool open = true;
             if (st.nb >= 32) {
-                drain_b(st, Q, A, lane);
+                drain_b<false, G>(st, Q, A, lane, &grp);
                 open = st.count <= 1;
             }
-            if (open) open = run_phase<true, false>(st, Q, A, lane);
-            if (open) open = run_phase<false, false>(st, Q, A, lane);
+            if (open) open = run_phase<true, false, G>(st, Q, A, lane, &grp);
+            if (open) open = run_phase<false, false, G>(st, Q, A, lane, &grp);
             while (open && st.na > 0) {
                 drain_a(st, Q, A, lane);
-                if (st.nb >= 32) { drain_b(st, Q, A, lane); open = st.count <= 1; }
+                if (st.nb >= 32) { drain_b<false, G>(st, Q, A, lane, &grp); open = st.count <= 1; }
             }
             while (open && st.nb > 0) {
-                drain_b(st, Q, A, lane);
+                drain_b<false, G>(st, Q, A, lane, &grp);
                 open = st.count <= 1;
             }
             group_bar(bar, nthr);
@@ -823,6 +871,22 @@ __global__ void __launch_bounds__(W * 32) search_kernel_group(const SearchArgs A
 }
 
 }  // namespace
+
+template <int W, bool kMR, int K>
+int launch_w(const SearchArgs& a, int sms, cudaStream_t stream)
+{
+    int per_sm = 0;
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel<W, kMR, K>, W * 32, 0));
+    if (per_sm < 1) per_sm = 1;
+    const uint32_t chunks = a.nseg ? a.nchunks : (a.nsums + K - 1) / K;
+    uint32_t blocks = (uint32_t)sms * (uint32_t)per_sm;
+    const uint32_t need = (chunks + W - 1) / W;
+    if (blocks > need) blocks = need;
+    if (blocks == 0) return 0;
+    search_kernel<W, kMR, K><<<blocks, W * 32, 0, stream>>>(a);
+    FFB_CUDA(cudaGetLastError());
+    return 0;
+}
 
 template <int W, int G>
 int launch_group(const SearchArgs& a, int sms, cudaStream_t stream)
@@ -840,53 +904,63 @@ int launch_group(const SearchArgs& a, int sms, cudaStream_t stream)
     return 0;
 }
 
-template <int W, bool kMR>
-int launch_w(const SearchArgs& a, int sms, cudaStream_t stream)
+template <int W>
+int launch_map_only(const SearchArgs& a, int sms, cudaStream_t stream)
 {
-    int per_sm = 0;
-    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel<W, kMR>, W * 32, 0));
-    if (per_sm < 1) per_sm = 1;
-    const uint32_t chunks = a.nseg ? a.nchunks : (a.nsums + a.chunk - 1) / a.chunk;
-    uint32_t blocks = (uint32_t)sms * (uint32_t)per_sm;
-    const uint32_t need = (chunks + W - 1) / W;
-    if (blocks > need) blocks = need;
-    if (blocks == 0) return 0;
-    search_kernel<W, kMR><<<blocks, W * 32, 0, stream>>>(a);
-    FFB_CUDA(cudaGetLastError());
-    return 0;
+    switch (a.chunk) {
+    case 16: return launch_w<W, false, 16>(a, sms, stream);
+    case 64: return launch_w<W, false, 64>(a, sms, stream);
+    default: return launch_w<W, false, 32>(a, sms, stream);
+    }
 }
 
 // The map-only kernel when the map reaches every value the sums up to a.hi probe (nothing
-// goes to Miller-Rabin in stages 0 and 1), else the variant that batches Miller-Rabin.
+// goes to Miller-Rabin in stages 0 and 1), else the variant that batches Miller-Rabin (32
+// sums per chunk, one warp per sum). Shapes outside the offered ones are refused.
 int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
 {
     if (a.nseg == 0 && a.nsums == 0) return 0;
     const uint64_t pb = ffb_probe_bound(a.hi);
     const bool mr = pb == 0 || a.bound < pb;
-    if (a.group != 1) {
-        // several warps per sum: map-only variant, chunks of 32 sums per warp of the group
-        if ((a.group != 2 && a.group != 4) || a.chunk != 32 * a.group || mr) {
-            std::fprintf(stderr, "ffb: %u warps per sum needs chunks of %u sums and a map over "
-                         "every probe\n", a.group, 32 * a.group);
-            return -1;
-        }
-        switch (a.warps) {
-        case 4: return a.group == 2 ? launch_group<4, 2>(a, sms, stream) : launch_group<4, 4>(a, sms, stream);
-        case 8: return a.group == 2 ? launch_group<8, 2>(a, sms, stream) : launch_group<8, 4>(a, sms, stream);
-        default: return a.group == 2 ? launch_group<16, 2>(a, sms, stream) : launch_group<16, 4>(a, sms, stream);
-        }
-    }
-    if (a.chunk != 16 && a.chunk != 32 && a.chunk != 64) {
-        std::fprintf(stderr, "ffb: search chunk of %u sums (16, 32 or 64)\n", a.chunk);
+    const bool warps_ok = a.warps == 0 || a.warps == 4 || a.warps == 8 || a.warps == 16;
+    const bool shape_ok = a.group == 1 ? (a.chunk == 32 || (!mr && (a.chunk == 16 || a.chunk == 64)))
+                                       : ((a.group == 2 || a.group == 4) && a.chunk == 32 * a.group && !mr);
+    if (!warps_ok || !shape_ok) {
+        std::fprintf(stderr, "ffb: search shape (%u warps a block, %u per sum, %u sums a chunk) not "
+                     "offered%s\n", a.warps, a.group, a.chunk,
+                     mr ? " with a map below the probes (one warp per sum, 32 sums a chunk)" : "");
         return -1;
     }
+    if (a.warps == 0 && a.group == 1 && a.chunk == 32 && a.nseg == 0 && !mr) {
+        // unset shape on one range over a map covering every probe: 16 warps a block, 2 per
+        // sum, 64-sum chunks (2^21 job on one box: 225 ms, against 230 ms for the best one-warp
+        // shape, 8 warps with 16-sum chunks, and 236 ms for 8 warps with 32-sum chunks)
+        SearchArgs b = a;
+        b.warps = 16;
+        b.group = 2;
+        b.chunk = 64;
+        return launch_group<16, 2>(b, sms, stream);
+    }
+    if (a.group == 2 || a.group == 4) {
+        switch (a.warps) {
+        case 4: return a.group == 2 ? launch_group<4, 2>(a, sms, stream) : launch_group<4, 4>(a, sms, stream);
+        case 16: return a.group == 2 ? launch_group<16, 2>(a, sms, stream) : launch_group<16, 4>(a, sms, stream);
+        default: return a.group == 2 ? launch_group<8, 2>(a, sms, stream) : launch_group<8, 4>(a, sms, stream);
+        }
+    }
+    if (mr) {
+        switch (a.warps) {
+        case 4: return launch_w<4, true, 32>(a, sms, stream);
+        case 16: return launch_w<16, true, 32>(a, sms, stream);
+        default: return launch_w<8, true, 32>(a, sms, stream);   // unset: 8 (the served mode's best)
+        }
+    }
     switch (a.warps) {
-    case 4: return mr ? launch_w<4, true>(a, sms, stream) : launch_w<4, false>(a, sms, stream);
-    case 8: return mr ? launch_w<8, true>(a, sms, stream) : launch_w<8, false>(a, sms, stream);
-    case 16: return mr ? launch_w<16, true>(a, sms, stream) : launch_w<16, false>(a, sms, stream);
-    // unset: the fastest measured block size of each variant (2^21 job: map-only 227 ms with
-    // 16 warps, 231 ms with 4, 247 ms with 8; served: the Miller-Rabin variant best with 8)
-    default: return mr ? launch_w<8, true>(a, sms, stream) : launch_w<16, false>(a, sms, stream);
+    case 4: return launch_map_only<4>(a, sms, stream);
+    case 16: return launch_map_only<16>(a, sms, stream);
+    // unset (a work queue, or a chunk given): 8 warps (2^21 job on one box: 236 ms with 8-warp
+    // blocks, 242 ms with 4, 319 ms with 16)
+    default: return launch_map_only<8>(a, sms, stream);
     }
 }
 

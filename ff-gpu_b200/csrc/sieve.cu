@@ -16,9 +16,9 @@
 // kernel and every other entry through sieve_generic.
 //
 // sieve_tiles (persistent grid over shared-memory tiles):
-//   1. A tile starts as the AND of three pre-computed patterns (the odd numbers free of
-//      3..13, of 17,19,23 and of 29,31,37; periods 15015, 7429 and 33263 odd numbers), read
-//      with funnel shifts at 32-bit phases advanced incrementally per word.
+//   1. A tile starts as the AND of eight pre-computed patterns (the odd numbers free of
+//      3..13, of 17,19,23, of 29,31,37 and of the pairs 41*43 .. 73*79), read with funnel
+//      shifts at 32-bit phases advanced incrementally per word: no prime up to 79 is marked.
 //   2. Small primes (p <= tile bits / 1024, at least 32 marks per lane): the "comb". The warp
 //      takes one prime; at each step its 32 lanes mark the multiples f + p*(r + 32*lane + 1024*t)
 //      for the same r, which lie 32p bits = p words apart: the same bit of 32 words whose
@@ -28,7 +28,7 @@
 //      30 only (the mod-30 wheel: steps of 3p, 2p, p, 2p, p, 2p, 3p, p bits). The multiples
 //      with k divisible by 3 or 5 are multiples of 3 or 5, already cleared by the patterns,
 //      so 7 of every 15 odd multiples are never marked. (Without the patterns, a caller list
-//      that lacks 3..37, every odd multiple is stepped.)
+//      that lacks 3..79, every odd multiple is stepped.)
 //   Warps take comb primes (smallest first) and groups of 32 larger primes from per-tile
 //   shared counters, so a warp that finishes early takes more work.
 //   4. The tile is converted to the reference bit order (brev + byte swap) and written to
@@ -45,7 +45,7 @@ namespace ffb {
 
 // Device-side description of the marking list (written by list_primes or uploaded):
 // primes [0, n) ascending; [ibeg, icomb) are comb primes, [icomb, n) one thread each
-// (ibeg skips the pattern primes 3..37 when the patterns are applied).
+// (ibeg skips the pattern primes 3..79 when the patterns are applied).
 struct SieveListHeader {
     uint32_t n, ibeg, icomb, pad;
 };
@@ -56,19 +56,38 @@ constexpr int kSieveThreads = 512;
 constexpr int kListThreads = 1024;
 constexpr uint32_t kListSegWords = 8192;   // list_primes segment: 262,144 odd values
 
-// Pre-sieve patterns: bit j (LSB-first) of pattern t is 1 iff the odd number 2j+1 has no
-// factor among the primes of group t; each pattern repeats with the product of its
-// primes (in odd numbers) and is stored with one extra period word so any 32-bit window
-// can be read without wrapping.
+// Pre-sieve patterns: bit j (LSB-first) of pattern g is 1 iff the odd number 2j+1 has no
+// factor among the primes of group g; each pattern repeats with the product of its primes (in
+// odd numbers) and is stored with one extra period word so any 32-bit window can be read
+// without wrapping. Groups 0..2 cover 3..37 (list_primes uses those three), groups 3..7 the
+// pairs 41*43, 47*53, 59*61, 67*71, 73*79: a pattern costs a few instructions per 32-bit word,
+// far less than the shared-memory atomics the marks of those primes would cost.
+constexpr int kGroups = 8;
 constexpr uint32_t kPeriod0 = 3 * 5 * 7 * 11 * 13;   // 15015
 constexpr uint32_t kPeriod1 = 17 * 19 * 23;          // 7429
 constexpr uint32_t kPeriod2 = 29 * 31 * 37;          // 33263
-constexpr uint32_t kWords0 = (kPeriod0 + 63) / 32 + 1;
-constexpr uint32_t kWords1 = (kPeriod1 + 63) / 32 + 1;
-constexpr uint32_t kWords2 = (kPeriod2 + 63) / 32 + 1;
-constexpr uint32_t kWheelWords = kWords0 + kWords1 + kWords2;
-constexpr int kWheelPrimes = 11;                     // 3 .. 37
+constexpr uint32_t kPeriod3 = 41 * 43, kPeriod4 = 47 * 53, kPeriod5 = 59 * 61,
+                   kPeriod6 = 67 * 71, kPeriod7 = 73 * 79;
+__host__ __device__ constexpr uint32_t words_of(uint32_t period) { return (period + 63) / 32 + 1; }
+constexpr uint32_t kWords0 = words_of(kPeriod0);
+constexpr uint32_t kWords1 = words_of(kPeriod1);
+constexpr uint32_t kWords2 = words_of(kPeriod2);
+constexpr uint32_t kWheelWords = kWords0 + kWords1 + kWords2 + words_of(kPeriod3) +
+                                 words_of(kPeriod4) + words_of(kPeriod5) + words_of(kPeriod6) +
+                                 words_of(kPeriod7);
+constexpr int kWheelPrimes = 21;                     // 3 .. 79
+constexpr uint32_t kLastPatternPrime = 79;
 __device__ uint32_t g_wheel[kWheelWords];
+
+__host__ __device__ constexpr uint32_t group_period(int g)
+{
+    return g == 0 ? kPeriod0 : g == 1 ? kPeriod1 : g == 2 ? kPeriod2 : g == 3 ? kPeriod3
+         : g == 4 ? kPeriod4 : g == 5 ? kPeriod5 : g == 6 ? kPeriod6 : kPeriod7;
+}
+__host__ __device__ constexpr uint32_t group_offset(int g)
+{
+    return g == 0 ? 0 : group_offset(g - 1) + words_of(group_period(g - 1));
+}
 
 // Steps of the mod-30 wheel in units of p bits, from the residues 1, 7, 11, 13, 17, 19, 23,
 // 29 of k (2 bits each, residue index 0 in the low bits), twice over so a 32-bit rotation
@@ -85,7 +104,7 @@ struct TileArgs {
     const uint32_t* primes; // marking list (device)
     const uint64_t* mu;     // floor((2^64-1) / p) per prime
     const SieveListHeader* hdr;
-    int wheel;              // the patterns are applied (the list holds 3..37)
+    int wheel;              // the patterns are applied (the list holds 3..79)
     int clear_one;          // clear the bit of the value 1 (seg_lo == 0)
     uint32_t tile_words;
     uint64_t ntiles;
@@ -94,6 +113,18 @@ struct TileArgs {
 __device__ __forceinline__ uint32_t window(const uint32_t* w, uint32_t ph)
 {
     return __funnelshift_r(w[ph >> 5], w[(ph >> 5) + 1], ph & 31);
+}
+
+// The 32-bit window of pattern g at phase ph, then ph advanced by `step` bits (a thread's
+// next word in the tile loop): offset, period and step are compile-time constants.
+template <int g, uint32_t step>
+__device__ __forceinline__ uint32_t pattern_word(const uint32_t* wheel, uint32_t& ph)
+{
+    constexpr uint32_t period = group_period(g), off = group_offset(g), adv = step % period;
+    const uint32_t x = window(wheel + off, ph);
+    ph += adv;
+    ph -= ph >= period ? period : 0;
+    return x;
 }
 
 // ~(1 << (x & 31)) in one funnel-shift rotation
@@ -144,20 +175,22 @@ __global__ void __launch_bounds__(kSieveThreads) sieve_tiles(const TileArgs A)
         if (threadIdx.x == 0) { ctr[0] = 0; ctr[1] = 0; }
         // ---- 1. initial pattern ----
         {
+            // the block is launched with kSieveThreads threads, so a thread's next word is
+            // 32 * kSieveThreads bits on: a compile-time phase step per pattern
             const uint64_t j = j0 + m0 + 32ull * threadIdx.x;
+            constexpr uint32_t adv = 32u * kSieveThreads;
             uint32_t ph0 = (uint32_t)(j % kPeriod0), ph1 = (uint32_t)(j % kPeriod1),
-                     ph2 = (uint32_t)(j % kPeriod2);
-            const uint32_t adv = 32u * blockDim.x;
-            const uint32_t s0 = adv % kPeriod0, s1 = adv % kPeriod1, s2 = adv % kPeriod2;
-            for (uint32_t w = threadIdx.x; w < words; w += blockDim.x) {
+                     ph2 = (uint32_t)(j % kPeriod2), ph3 = (uint32_t)(j % kPeriod3),
+                     ph4 = (uint32_t)(j % kPeriod4), ph5 = (uint32_t)(j % kPeriod5),
+                     ph6 = (uint32_t)(j % kPeriod6), ph7 = (uint32_t)(j % kPeriod7);
+            for (uint32_t w = threadIdx.x; w < words; w += kSieveThreads) {
                 const uint64_t gm = m0 + 32ull * w;
                 uint32_t x = 0xFFFFFFFFu;
                 if (A.wheel) {
-                    x = window(wheel, ph0) & window(wheel + kWords0, ph1) &
-                        window(wheel + kWords0 + kWords1, ph2);
-                    ph0 += s0; ph0 -= ph0 >= kPeriod0 ? kPeriod0 : 0;
-                    ph1 += s1; ph1 -= ph1 >= kPeriod1 ? kPeriod1 : 0;
-                    ph2 += s2; ph2 -= ph2 >= kPeriod2 ? kPeriod2 : 0;
+                    x = pattern_word<0, adv>(wheel, ph0) & pattern_word<1, adv>(wheel, ph1) &
+                        pattern_word<2, adv>(wheel, ph2) & pattern_word<3, adv>(wheel, ph3) &
+                        pattern_word<4, adv>(wheel, ph4) & pattern_word<5, adv>(wheel, ph5) &
+                        pattern_word<6, adv>(wheel, ph6) & pattern_word<7, adv>(wheel, ph7);
                 }
                 if (gm + 32 > A.nbits) {  // bits of values >= seg_hi stay set
                     const uint64_t keep = A.nbits > gm ? A.nbits - gm : 0;
@@ -226,8 +259,9 @@ __global__ void __launch_bounds__(kSieveThreads) sieve_tiles(const TileArgs A)
         }
         __syncthreads();
         // ---- the pattern primes themselves and the value 1 ----
-        if (threadIdx.x == 0 && A.base_odd <= 37) {
-            const uint32_t wp[kWheelPrimes] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+        if (threadIdx.x == 0 && A.base_odd <= kLastPatternPrime) {
+            const uint32_t wp[kWheelPrimes] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37,
+                                               41, 43, 47, 53, 59, 61, 67, 71, 73, 79};
             if (A.wheel)
                 for (int q = 0; q < kWheelPrimes; ++q) {
                     if (wp[q] < A.base_odd) continue;
@@ -350,8 +384,8 @@ __global__ void __launch_bounds__(kListThreads) list_primes(uint64_t L, uint32_t
                 x &= keep >= 32 ? 0xFFFFFFFFu : (1u << keep) - 1u;
             }
             if (b0 == 0 && w < 2) {  // the pattern primes 3..37 themselves (bits 0..17)
-                const uint32_t wp[kWheelPrimes] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
-                for (int q = 0; q < kWheelPrimes; ++q) {
+                const uint32_t wp[11] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+                for (int q = 0; q < 11; ++q) {
                     const uint32_t bb = (wp[q] - 3) / 2;
                     if (bb / 32 == w && bb < b1) x |= 1u << (bb & 31);
                 }
@@ -394,7 +428,7 @@ __global__ void __launch_bounds__(kListThreads) list_primes(uint64_t L, uint32_t
                     primes[pos] = (uint32_t)v;
                     mu[pos] = ~0ull / v;
                 }
-                if (v <= 37) atomicMax(&s_ibeg, pos + 1);
+                if (v <= kLastPatternPrime) atomicMax(&s_ibeg, pos + 1);
                 if (v <= pcomb) atomicMax(&s_icomb, pos + 1);
             }
             base += __popc(m);
@@ -436,18 +470,16 @@ int upload_wheel()
     FFB_CUDA(cudaGetDevice(&dev));
     if (done_dev == dev) return 0;
     std::vector<uint32_t> w(kWheelWords, 0);
-    const uint32_t periods[3] = {kPeriod0, kPeriod1, kPeriod2};
-    const uint32_t words[3] = {kWords0, kWords1, kWords2};
-    const uint32_t group[3][5] = {{3, 5, 7, 11, 13}, {17, 19, 23, 0, 0}, {29, 31, 37, 0, 0}};
-    uint32_t off = 0;
-    for (int g = 0; g < 3; ++g) {
-        for (uint32_t j = 0; j < words[g] * 32; ++j) {
-            const uint32_t v = 2 * (j % periods[g]) + 1;
+    const uint32_t group[kGroups][5] = {{3, 5, 7, 11, 13}, {17, 19, 23}, {29, 31, 37}, {41, 43},
+                                        {47, 53},          {59, 61},     {67, 71},     {73, 79}};
+    for (int g = 0; g < kGroups; ++g) {
+        const uint32_t off = group_offset(g), period = group_period(g);
+        for (uint32_t jj = 0; jj < words_of(period) * 32; ++jj) {
+            const uint32_t v = 2 * (jj % period) + 1;
             bool keep = true;
             for (int q = 0; q < 5 && group[g][q]; ++q) keep = keep && v % group[g][q] != 0;
-            if (keep) w[off + (j >> 5)] |= 1u << (j & 31);
+            if (keep) w[off + (jj >> 5)] |= 1u << (jj & 31);
         }
-        off += words[g];
     }
     FFB_CUDA(cudaMemcpyToSymbol(g_wheel, w.data(), w.size() * 4));
     done_dev = dev;
@@ -557,7 +589,7 @@ int analyse(const SieveArgs& a, int sms, SieveHost& H)
         // primes of the standard prefix with p*p < seg_hi mark something
         uint32_t iend = 0;
         while (iend < std_n && (uint64_t)h[off + iend] * h[off + iend] < a.seg_hi) ++iend;
-        wheel = std_n >= kWheelPrimes;  // the patterns need 3..37 in the list
+        wheel = std_n >= kWheelPrimes;  // the patterns need 3..79 in the list
         H.list.assign(h + off, h + off + iend);
         H.mu.resize(iend);
         for (uint32_t i = 0; i < iend; ++i) H.mu[i] = ~0ull / h[off + i];   // Barrett constants

@@ -207,10 +207,11 @@ int ffb_search_async(int deviceIndex, const uint8_t* d_map, uint64_t mapBound, u
                      uint32_t hi, uint64_t* d_rec, void* stream);
 
 /* ffb_search_async with an explicit launch shape (no reference counterpart): `warps` warps
- * per block (4, 8, 16), `group` warps per sum (1; or 2, 4 when the map covers every probe,
- * mapBound >= ffb_probe_bound(hi)) and `chunk` sums taken from the work counter at a time
- * (16, 32, 64 with one warp per sum; 32 * group otherwise). These are the candidates the
- * batch's autotuner times; every shape gives the same records. Other shapes return -1. */
+ * per block (4, 8, 16), `group` warps per sum (1, 2, 4) and `chunk` sums taken from the
+ * work counter at a time (16, 32, 64 with one warp per sum; 32 * group otherwise). Groups and
+ * chunks other than 32 need a map that covers every probe (mapBound >= ffb_probe_bound(hi)).
+ * These are the candidates the batch's autotuner times; every shape gives the same records.
+ * Other shapes return -1. */
 int ffb_search_shape_async(int deviceIndex, const uint8_t* d_map, uint64_t mapBound, uint32_t lo,
                            uint32_t hi, uint64_t* d_rec, uint32_t warps, uint32_t chunk,
                            uint32_t group, void* stream);
