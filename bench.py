@@ -47,7 +47,7 @@ LIMIT = 2097152
 METRIC = "sums/sec byte-identical at sumLimit=2^21; served p50/p99 latency vs plain"
 UNIT = "sums/s"
 NORM = re.compile(rb"(Prime|Freudenthal) time: [0-9]+")
-DEFAULT_TILE = 96 * 1024    # the sieve's shared-memory tile when the caller does not choose
+DEFAULT_TILE = 216 * 1024   # the sieve's shared-memory tile when the caller does not choose
 
 # Integer operations per occurrence of each primitive of the reference search, counted as
 # the 32-bit integer instructions (IMAD or ALU) an implementation needs:
@@ -161,12 +161,12 @@ def odd_primes_upto(n):
 
 def sieve_marks(mpv, tile_bytes):
     """Shared-memory marks sieve_tiles makes for the map of values 0..mpv: the comb primes
-    (83 <= p <= tile bits / 1024) mark every odd multiple from p^2, the larger primes the
+    (83 <= p <= tile bits / 2048) mark every odd multiple from p^2, the larger primes the
     multiples p*k, k >= p, with k prime to 30 (the patterns cover 3..79)."""
     import numpy as np
     p = odd_primes_upto(math.isqrt(mpv))
     p = p[p >= 83]
-    pcomb = tile_bytes * 8 // 1024
+    pcomb = tile_bytes * 8 // 2048
     comb = p[p <= pcomb]
     wheel = p[p > pcomb]
     n_comb = int(((mpv - comb * comb) // (2 * comb) + 1).sum())

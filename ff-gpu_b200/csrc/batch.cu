@@ -178,10 +178,10 @@ int autotune(FfbBatch* b)
             return build_queue(b) || build_sieve(b);
         }
     }
-    // the tile shares the CTA's 227 KB of shared memory with ~7 KB of pre-sieve patterns
+    // the tile shares the CTA's 227 KB of shared memory with ~9 KB of pre-sieve patterns
     const uint32_t tiles[] = {64 * 1024, 96 * 1024, 128 * 1024, 160 * 1024, 192 * 1024, 216 * 1024};
     float best = 1e30f;
-    uint32_t best_tile = 96 * 1024;
+    uint32_t best_tile = 216 * 1024;
     for (uint32_t t : tiles) {
         b->tile_bytes = t;
         if (build_sieve(b)) continue;  // a tile that does not fit is skipped
@@ -368,7 +368,7 @@ extern "C" FfbBatch* ffb_batch_create(int deviceIndex, uint32_t n, const int32_t
         ffb_batch_destroy(b);
         return nullptr;
     }
-    b->tile_bytes = 96 * 1024;
+    b->tile_bytes = 216 * 1024;
     b->warps = 8;
     if ((autotune_flag ? autotune(b) : build_sieve(b)) || capture(b)) {
         ffb_batch_destroy(b);

@@ -52,7 +52,7 @@ struct SieveListHeader {
 
 namespace {
 
-constexpr int kSieveThreads = 512;
+constexpr int kSieveThreads = 1024;
 constexpr int kListThreads = 1024;
 constexpr uint32_t kListSegWords = 8192;   // list_primes segment: 262,144 odd values
 
@@ -551,13 +551,13 @@ int analyse(const SieveArgs& a, int sms, SieveHost& H)
         std::fprintf(stderr, "ffb: sieve output must be 16-byte aligned\n");
         return -1;
     }
-    uint32_t tile_bytes = a.tile_bytes ? a.tile_bytes : 96 * 1024;
+    uint32_t tile_bytes = a.tile_bytes ? a.tile_bytes : 216 * 1024;
     tile_bytes = (tile_bytes + 15) & ~15u;
     TileArgs& T = H.T;
     T.tile_words = tile_bytes / 4;
     const uint64_t tile_bits = (uint64_t)T.tile_words * 32;
-    // comb primes: at least 1024 multiples per tile (32 per lane)
-    H.pcomb = (uint32_t)std::min<uint64_t>(tile_bits / 1024, 1u << 20);
+    // comb primes: at least 2048 multiples per tile (64 per lane)
+    H.pcomb = (uint32_t)std::min<uint64_t>(tile_bits / 2048, 1u << 20);
     int wheel = 1;
     if (a.true_map) {
         // the true map: odd primes p with p*p < seg_hi, made on the device

@@ -195,7 +195,7 @@ int ffb_sieve_map_async(int deviceIndex, uint64_t maxPrimeMapValue, uint8_t* d_m
                         void* stream);
 
 /* ffb_sieve_map_async with the shared-memory tile of the sieve given (1 KB..216 KB, a
- * multiple of 16; the default is 96 KB): the slab-size knob of the reference's engine
+ * multiple of 16; the default is 216 KB): the slab-size knob of the reference's engine
  * (--slab-size), for sweeps and tuning. */
 int ffb_sieve_map_tiled_async(int deviceIndex, uint64_t maxPrimeMapValue, uint8_t* d_map,
                               uint32_t tileBytes, void* stream);
