@@ -30,14 +30,44 @@
 namespace ffb {
 namespace {
 
+#ifndef FFB_SEARCH_WARPS_PER_SM
+#define FFB_SEARCH_WARPS_PER_SM 32
+#endif
+// Resident warps per SM the kernels' register budget is set for (64 registers a thread at 32
+// warps): the search waits on map reads, and more resident warps beat fewer spills.
+constexpr int kWarpsPerSm = FFB_SEARCH_WARPS_PER_SM;
 constexpr int kQueue = 64;       // per-warp queue capacity (entries)
-constexpr int kMaxPf = 16;       // distinct odd prime factors of a product < 2^52
 constexpr int kMaxDiv = 64;      // divisor list of one AllButOne... call (Miller-Rabin variant)
 
+// Stage 2 works in a per-lane scratch of shared memory (no local memory): word j of a lane
+// lies at [32 j + lane] of its warp's area, so a lane always reads its own bank.
+//   words 0 .. kFacSlots-1    the product's prime powers, ascending, q | e << 27 (the terms
+//                             are below 2^25, so q < 2^27 and e < 32)
+//   words kFacSlots ..        the odometer's partial divisors Sd[0..n] in all_but_one, and
+//                             the factors of the second term while the product is factored
+// A product below 2^50 has at most 12 distinct odd primes (3*5*...*43 > 2^50); one slot more
+// shows an overflow, which is reported as kErrFactorList.
+constexpr int kFacSlots = 13;
+constexpr int kSdSlots = 13;
+constexpr uint32_t kWarpScratchWords = 32 * (kFacSlots + kSdSlots);
+constexpr uint32_t kWarpScratchBytes = 4 * kWarpScratchWords;
+
+__device__ __forceinline__ uint32_t* lane_scratch()
+{
+    extern __shared__ uint32_t search_scratch[];
+    return search_scratch + (threadIdx.x >> 5) * kWarpScratchWords + (threadIdx.x & 31);
+}
+
+__device__ __forceinline__ uint32_t fac_word(uint32_t q, uint32_t e) { return q | e << 27; }
+__device__ __forceinline__ uint32_t fac_q(uint32_t w) { return w & 0x07FFFFFFu; }
+__device__ __forceinline__ uint32_t fac_e(uint32_t w) { return w >> 27; }
+
+// A product's factorisation in a lane's scratch: n distinct primes (n > kFacSlots: overflow).
 struct Fac {
-    uint32_t q[kMaxPf];
-    uint32_t e[kMaxPf];
+    uint32_t* w;
     int n;
+    __device__ uint32_t q(int i) const { return fac_q(w[32 * i]); }
+    __device__ uint32_t e(int i) const { return fac_e(w[32 * i]); }
 };
 
 // Prime::IsPrime for the search (reference/segmentedSieve.C:283-296), for the values that
@@ -84,14 +114,14 @@ __device__ __forceinline__ int pair_class(const SearchArgs& A, uint64_t i)
 }
 
 // Ascending prime factorisation of an odd x < 2^32 by the exact-division table, with the
-// cofactor's primality read from the bitmap after every factor found.
-template <bool kMR>
-__device__ int factor_odd(uint32_t x, uint32_t* q, uint32_t* e, int cap, const SearchArgs& A)
+// cofactor's primality read from the bitmap after every factor found: put(q, e) receives
+// the prime powers in ascending order.
+template <bool kMR, class Put>
+__device__ __forceinline__ void factor_odd(uint32_t x, const SearchArgs& A, Put&& put)
 {
-    int cnt = 0;
     uint32_t n = x;
-    if (n <= 1) return 0;
-    if (isp<kMR>(A, n)) { q[0] = n; e[0] = 1; return 1; }
+    if (n <= 1) return;
+    if (isp<kMR>(A, n)) { put(n, 1u); return; }
     for (uint32_t i = 0; i < A.ntdiv; ++i) {
         const TDiv t = A.tdiv[i];
         if ((uint64_t)t.p * t.p > n) break;
@@ -99,38 +129,39 @@ __device__ int factor_odd(uint32_t x, uint32_t* q, uint32_t* e, int cap, const S
         if (y <= t.lim) {
             uint32_t ex = 0;
             do { n = y; ++ex; y = n * t.inv; } while (y <= t.lim);
-            if (cnt < cap) { q[cnt] = t.p; e[cnt] = ex; }
-            ++cnt;
-            if (n == 1) return cnt;
-            if (isp<kMR>(A, n)) {
-                if (cnt < cap) { q[cnt] = n; e[cnt] = 1; }
-                return cnt + 1;
-            }
+            put(t.p, ex);
+            if (n == 1) return;
+            if (isp<kMR>(A, n)) { put(n, 1u); return; }
         }
     }
-    if (n > 1) {
-        if (cnt < cap) { q[cnt] = n; e[cnt] = 1; }
-        ++cnt;
-    }
-    return cnt;
+    if (n > 1) put(n, 1u);
 }
 
+// The factorisation of a*b (a, b odd) into the lane's scratch L: b's prime powers first go
+// to the odometer words, then a's are merged with them on the fly (both lists ascend).
 template <bool kMR>
-__device__ void factor_product(uint32_t a, uint32_t b, Fac& f, const SearchArgs& A)
+__device__ __forceinline__ Fac factor_product(uint32_t a, uint32_t b, uint32_t* L, const SearchArgs& A)
 {
-    uint32_t qa[10], ea[10], qb[10], eb[10];
-    int na = factor_odd<kMR>(a, qa, ea, 10, A);
-    int nb = b == 1 ? 0 : factor_odd<kMR>(b, qb, eb, 10, A);
-    int i = 0, j = 0, n = 0;
-    while (i < na || j < nb) {
-        uint32_t q, e;
-        if (j >= nb || (i < na && qa[i] < qb[j])) { q = qa[i]; e = ea[i]; ++i; }
-        else if (i >= na || qb[j] < qa[i]) { q = qb[j]; e = eb[j]; ++j; }
-        else { q = qa[i]; e = ea[i] + eb[j]; ++i; ++j; }
-        if (n < kMaxPf) { f.q[n] = q; f.e[n] = e; }
+    uint32_t* fb = L + 32 * kFacSlots;
+    int nb = 0;
+    if (b > 1)
+        factor_odd<kMR>(b, A, [&](uint32_t q, uint32_t e) {
+            if (nb < kSdSlots) fb[32 * nb] = fac_word(q, e);
+            ++nb;
+        });
+    if (nb > kSdSlots) nb = kSdSlots;  // (b < 2^25 has at most 7 distinct odd primes)
+    int j = 0, n = 0;
+    auto put = [&](uint32_t w) {
+        if (n < kFacSlots) L[32 * n] = w;
         ++n;
-    }
-    f.n = n < kMaxPf ? n : kMaxPf;
+    };
+    factor_odd<kMR>(a, A, [&](uint32_t q, uint32_t e) {
+        for (; j < nb && fac_q(fb[32 * j]) < q; ++j) put(fb[32 * j]);
+        if (j < nb && fac_q(fb[32 * j]) == q) e += fac_e(fb[32 * j++]);
+        put(fac_word(q, e));
+    });
+    for (; j < nb; ++j) put(fb[32 * j]);
+    return Fac{L, n};
 }
 
 // x / d for an odd d that divides x: x times the inverse of d modulo 2^64 (Newton's
@@ -154,37 +185,40 @@ __device__ __forceinline__ uint64_t exact_quotient(uint64_t x, uint32_t d)
 // with an odometer over the exponents (digit i counts the power of factor i, 5 bits each; a
 // digit that cannot grow without passing lim is reset and the next one grows), keeping per
 // digit the divisor made of the digits from i up; the cofactor oddProduct/d is an exact
-// division by d's inverse modulo 2^64. No divisor list is stored.
+// division by d's inverse modulo 2^64. No divisor list is stored (the partial divisors sit
+// in the lane's shared scratch). Inlined: as an out-of-line call its caller saved and restored
+// some 500 bytes of registers per thread around it (2^21 job: 207 ms inlined, 222 ms not).
 template <bool kMR>
-__device__ __noinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const Fac& f,
-                                         const SearchArgs& A)
+__device__ __forceinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const Fac f,
+                                            const SearchArgs& A)
 {
     const uint64_t P = odd_product << k;
     const uint64_t lim = isqrt64(P);
     uint32_t nm = 0;
     if ((1ull << k) <= lim) nm += !pair1<kMR>(A, (1ull << k) + odd_product);
     const int n = f.n;
-    if (n > 12) {   // 12 digits of 5 bits fill the odometer; products < 2^48 have at most 12
+    if (n > 12) {   // 12 digits of 5 bits fill the odometer; products < 2^50 have at most 12
         atomicOr(A.err, kErrFactorList);
         return false;
     }
-    uint32_t Sd[kMaxPf + 1];
+    uint32_t* Sd = f.w + 32 * kFacSlots;   // Sd[j] at Sd[32 j]: the lane's odometer words
     uint64_t ex = 0;
-    for (int j = 0; j <= n; ++j) Sd[j] = 1;
+    for (int j = 0; j <= n; ++j) Sd[32 * j] = 1;
     for (;;) {
         int i = 0;
         uint32_t q = 0;
         for (; i < n; ++i) {
-            q = f.q[i];
-            const uint32_t e = f.e[i], a = (uint32_t)(ex >> (5 * i)) & 31;
-            if (a < e && (uint64_t)Sd[i] * q <= lim) break;
+            const uint32_t w = f.w[32 * i];
+            q = fac_q(w);
+            const uint32_t e = fac_e(w), a = (uint32_t)(ex >> (5 * i)) & 31;
+            if (a < e && (uint64_t)Sd[32 * i] * q <= lim) break;
             ex &= ~(31ull << (5 * i));
-            Sd[i] = Sd[i + 1];
+            Sd[32 * i] = Sd[32 * (i + 1)];
         }
         if (i == n) break;
         ex += 1ull << (5 * i);
-        const uint32_t d = Sd[i] * q;
-        for (int j = 0; j <= i; ++j) Sd[j] = d;
+        const uint32_t d = Sd[32 * i] * q;
+        for (int j = 0; j <= i; ++j) Sd[32 * j] = d;
         const uint64_t c = exact_quotient(odd_product, d);
         if ((nm += !pair1<kMR>(A, d + (c << k))) > 1) return false;
         if (((uint64_t)d << k) <= lim && (nm += !pair1<kMR>(A, ((uint64_t)d << k) + c)) > 1)
@@ -199,7 +233,7 @@ __device__ __noinline__ bool all_but_one(uint32_t k, uint64_t odd_product, const
 // count of pairs already known not to be single (2 once the verdict is "no"); the verdict is
 // "yes" iff that count plus the pending probes found composite is exactly 1 (the order of the
 // tests does not change it). *np receives the number of pending pair sums.
-__device__ __noinline__ uint32_t all_but_one_defer(uint32_t k, uint64_t odd_product, const Fac& f,
+__device__ __noinline__ uint32_t all_but_one_defer(uint32_t k, uint64_t odd_product, const Fac f,
                                                    const SearchArgs& A, uint64_t* pend,
                                                    uint32_t* np)
 {
@@ -208,6 +242,10 @@ __device__ __noinline__ uint32_t all_but_one_defer(uint32_t k, uint64_t odd_prod
     uint64_t F[kMaxDiv], C[kMaxDiv];
     uint32_t nf = 0, npend = 0, nm = 0, nd = 0;
     *np = 0;
+    if (f.n > kFacSlots - 1) {   // more primes than the scratch holds: never for terms < 2^25
+        atomicOr(A.err, kErrFactorList);
+        return 2;
+    }
     // counts a pair sum: 0 not single, 1 single, 2 pending; returns true once nm > 1
     auto visit = [&](uint64_t v) {
         const int c = pair_class(A, v);
@@ -228,12 +266,12 @@ __device__ __noinline__ uint32_t all_but_one_defer(uint32_t k, uint64_t odd_prod
         uint32_t e;
         if (first) {
             first = false;
-            if (f.n > 0 && f.q[0] == 3) { q = 3; e = f.e[0]; idx = 1; }
+            if (f.n > 0 && f.q(0) == 3) { q = 3; e = f.e(0); idx = 1; }
             else continue;
         } else {
             if (idx >= f.n) break;                                   // testProduct == 1
-            q = f.q[idx];
-            e = f.e[idx];
+            q = f.q(idx);
+            e = f.e(idx);
             if (idx == f.n - 1 && e == 1 && q > lim) break;          // prime cofactor > limit
             ++idx;
         }
@@ -279,28 +317,36 @@ __device__ __forceinline__ uint32_t enc(uint32_t k, uint32_t o, bool comp)
     return k | (comp ? 32u : 0u) | (o << 6);
 }
 
+// The terms of a stage-2 item and the factorisation of their odd product (in the lane's
+// scratch). Power2Composite items (bit 5) pair 2^k with the odd term s - 2^k.
+template <bool kMR>
+__device__ __forceinline__ Fac stage2_terms(uint32_t item, uint32_t s, const SearchArgs& A,
+                                            uint32_t* ta, uint32_t* tb, uint64_t* odd_product)
+{
+    const uint32_t k = item & 31;
+    uint32_t* L = lane_scratch();
+    if (item & 32) {
+        const uint32_t odd = s - (1u << k);
+        *odd_product = odd;
+        *ta = 1u << k;
+        *tb = odd;
+        return factor_product<kMR>(odd, 1, L, A);
+    }
+    const uint32_t o = item >> 6;
+    const uint32_t even = o << k, b = s - even;
+    *odd_product = (uint64_t)o * b;
+    *ta = even;
+    *tb = b;
+    return factor_product<kMR>(o, b, L, A);
+}
+
 // Stage 2: the split's AllButOne... verdict (DoesPeterKnow's last step, or Power2Composite).
 template <bool kMR>
 __device__ bool stage2(uint32_t item, uint32_t s, const SearchArgs& A, uint32_t* ta, uint32_t* tb)
 {
-    const uint32_t k = item & 31;
-    Fac f;
     uint64_t odd_product;
-    if (item & 32) {
-        const uint32_t odd = s - (1u << k);
-        factor_product<kMR>(odd, 1, f, A);
-        odd_product = odd;
-        *ta = 1u << k;
-        *tb = odd;
-    } else {
-        const uint32_t o = item >> 6;
-        const uint32_t even = o << k, b = s - even;
-        factor_product<kMR>(o, b, f, A);
-        odd_product = (uint64_t)o * b;
-        *ta = even;
-        *tb = b;
-    }
-    return all_but_one<kMR>(k, odd_product, f, A);
+    const Fac f = stage2_terms<kMR>(item, s, A, ta, tb, &odd_product);
+    return all_but_one<kMR>(item & 31, odd_product, f, A);
 }
 
 // Stage 2 of the Miller-Rabin variant: the factorisation and the divisor pairs, with the
@@ -308,24 +354,9 @@ __device__ bool stage2(uint32_t item, uint32_t s, const SearchArgs& A, uint32_t*
 __device__ uint32_t stage2_defer(uint32_t item, uint32_t s, const SearchArgs& A, uint32_t* ta,
                                  uint32_t* tb, uint64_t* pend, uint32_t* np)
 {
-    const uint32_t k = item & 31;
-    Fac f;
     uint64_t odd_product;
-    if (item & 32) {
-        const uint32_t odd = s - (1u << k);
-        factor_product<true>(odd, 1, f, A);
-        odd_product = odd;
-        *ta = 1u << k;
-        *tb = odd;
-    } else {
-        const uint32_t o = item >> 6;
-        const uint32_t even = o << k, b = s - even;
-        factor_product<true>(o, b, f, A);
-        odd_product = (uint64_t)o * b;
-        *ta = even;
-        *tb = b;
-    }
-    return all_but_one_defer(k, odd_product, f, A, pend, np);
+    const Fac f = stage2_terms<true>(item, s, A, ta, tb, &odd_product);
+    return all_but_one_defer(item & 31, odd_product, f, A, pend, np);
 }
 
 // Stage 1: the pair sum 2^k + o*b whose probe 2^k + o*b - 2 is DoesPeterKnow's first test.
@@ -530,23 +561,27 @@ template <bool kOdd, bool kMR>
 __device__ __forceinline__ int stage0(uint32_t s, uint32_t k, uint32_t o, bool act,
                                       const SearchArgs& A)
 {
-    // Both map reads are issued before any branch (the probe is clamped into the map, and
-    // b is only read for an active lane), so the two splits a lane holds per step overlap
-    // their latency. b = s - o*2^k is odd and below s; v = o + b*2^k is odd, so the probe of
-    // single_pair(v) is v - 2.
+    // The divisibility filters come first and the probe's map word is read only for a split
+    // that passes them (a random sector of the map: most of the search's DRAM traffic); the
+    // reads of the two splits a lane holds per step are still issued before either is used.
+    // b = s - o*2^k is odd and below s (its bit lies in the cache-resident prefix of the map);
+    // v = o + b*2^k is odd, so the probe of single_pair(v) is v - 2.
     const uint32_t b = act ? s - (o << k) : 1;
     const uint64_t v = o + ((uint64_t)b << k);
     const uint64_t n = v - 2;
-    const uint64_t nr = n <= A.bound ? n : 1;
-    const uint32_t mv = __ldg(A.map + (nr >> 4));
     bool pre;
+    uint32_t mv = 0;
     if (kOdd) {
-        pre = o % 3 != 0 && b % 3 != 0;
+        pre = act && o % 3 != 0 && b % 3 != 0;
+        if (pre && n <= A.bound) mv = __ldg(A.map + (n >> 4));
     } else {
-        const uint32_t mb = __ldg(A.map + (b >> 4));
-        pre = o % 3 == 0 || b % 3 == 0 || ((mb >> (7 - ((b >> 1) & 7))) & 1);
+        const bool m3 = o % 3 == 0 || b % 3 == 0;
+        // the b-prime case (no multiple of 3) reads the probe after b's bit: rare
+        if (act && m3 && n <= A.bound) mv = __ldg(A.map + (n >> 4));
+        pre = act && (m3 || ((__ldg(A.map + (b >> 4)) >> (7 - ((b >> 1) & 7))) & 1));
+        if (pre && !m3 && n <= A.bound) mv = __ldg(A.map + (n >> 4));
     }
-    if (!act || !pre) return 0;
+    if (!pre) return 0;
     if (o == b) return 1;
     if (n > A.bound) {
         if constexpr (kMR) return pair_class(A, v);
@@ -620,9 +655,9 @@ __device__ void write_result(const SearchArgs& A, uint32_t s, uint32_t ri, uint3
 }
 
 template <int W, bool kMR, int K>
-__global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
+__device__ __forceinline__ void search_body(const SearchArgs& A)
 {
-    static_assert(K == 16 || K == 32 || K == 64, "sums per chunk");
+    static_assert(K == 8 || K == 16 || K == 32 || K == 64, "sums per chunk");
     __shared__ WarpQ<kMR> queues[W];
     const int lane = threadIdx.x & 31;
     WarpQ<kMR>& Q = queues[threadIdx.x >> 5];
@@ -732,6 +767,20 @@ __global__ void __launch_bounds__(W * 32) search_kernel(const SearchArgs A)
 }
 
 
+// The map-only kernel keeps kWarpsPerSm warps resident (its register budget follows); the
+// Miller-Rabin variant, whose deferred divisor lists are larger, keeps the compiler's own.
+template <int W, int K>
+__global__ void __launch_bounds__(W * 32, kWarpsPerSm / W) search_kernel(const SearchArgs A)
+{
+    search_body<W, false, K>(A);
+}
+
+template <int W>
+__global__ void __launch_bounds__(W * 32) search_kernel_mr(const SearchArgs A)
+{
+    search_body<W, true, 32>(A);
+}
+
 // Several warps on one sum (map-only variant): a group of G warps takes chunks of 32*G sums;
 // each warp runs the lane-parallel filter on 32 of them and appends its survivors to the
 // group's list, then the G warps take the survivors one at a time, each enumerating every
@@ -752,7 +801,7 @@ __device__ __forceinline__ void group_bar(uint32_t id, uint32_t threads)
 }
 
 template <int W, int G>
-__global__ void __launch_bounds__(W * 32) search_kernel_group(const SearchArgs A)
+__global__ void __launch_bounds__(W * 32, kWarpsPerSm / W) search_kernel_group(const SearchArgs A)
 {
     static_assert(G > 1 && W % G == 0 && W / G <= 15, "group shape");
     __shared__ WarpQ<false> queues[W];
@@ -872,18 +921,24 @@ __global__ void __launch_bounds__(W * 32) search_kernel_group(const SearchArgs A
 
 }  // namespace
 
+// The stage-2 scratch is dynamic shared memory, W * 3.3 KB a block (above the 48 KB a block
+// gets without asking for 16 warps); the attribute is set at every launch, which stream
+// capture allows.
 template <int W, bool kMR, int K>
 int launch_w(const SearchArgs& a, int sms, cudaStream_t stream)
 {
+    void (*kernel)(SearchArgs) = kMR ? search_kernel_mr<W> : search_kernel<W, K>;
+    const uint32_t dyn = W * kWarpScratchBytes;
+    FFB_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     int per_sm = 0;
-    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel<W, kMR, K>, W * 32, 0));
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, W * 32, dyn));
     if (per_sm < 1) per_sm = 1;
     const uint32_t chunks = a.nseg ? a.nchunks : (a.nsums + K - 1) / K;
     uint32_t blocks = (uint32_t)sms * (uint32_t)per_sm;
     const uint32_t need = (chunks + W - 1) / W;
     if (blocks > need) blocks = need;
     if (blocks == 0) return 0;
-    search_kernel<W, kMR, K><<<blocks, W * 32, 0, stream>>>(a);
+    kernel<<<blocks, W * 32, dyn, stream>>>(a);
     FFB_CUDA(cudaGetLastError());
     return 0;
 }
@@ -891,15 +946,17 @@ int launch_w(const SearchArgs& a, int sms, cudaStream_t stream)
 template <int W, int G>
 int launch_group(const SearchArgs& a, int sms, cudaStream_t stream)
 {
+    const uint32_t dyn = W * kWarpScratchBytes;
+    FFB_CUDA(cudaFuncSetAttribute(search_kernel_group<W, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
     int per_sm = 0;
-    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel_group<W, G>, W * 32, 0));
+    FFB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, search_kernel_group<W, G>, W * 32, dyn));
     if (per_sm < 1) per_sm = 1;
     const uint32_t chunks = a.nseg ? a.nchunks : (a.nsums + 32 * G - 1) / (32 * G);
     uint32_t blocks = (uint32_t)sms * (uint32_t)per_sm;
     const uint32_t need = (chunks + W / G - 1) / (W / G);
     if (blocks > need) blocks = need;
     if (blocks == 0) return 0;
-    search_kernel_group<W, G><<<blocks, W * 32, 0, stream>>>(a);
+    search_kernel_group<W, G><<<blocks, W * 32, dyn, stream>>>(a);
     FFB_CUDA(cudaGetLastError());
     return 0;
 }
@@ -932,14 +989,13 @@ int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
         return -1;
     }
     if (a.warps == 0 && a.group == 1 && a.chunk == 32 && a.nseg == 0 && !mr) {
-        // unset shape on one range over a map covering every probe: 16 warps a block, 2 per
-        // sum, 64-sum chunks (2^21 job on one box: 225 ms, against 230 ms for the best one-warp
-        // shape, 8 warps with 16-sum chunks, and 236 ms for 8 warps with 32-sum chunks)
+        // unset shape on one range over a map covering every probe: 16 warps a block, one per
+        // sum, 8-sum chunks (2^21 job on one box: 202.5 ms; 16-sum chunks 203-206 ms, 4 or 8
+        // warps the same, 32-sum chunks 213 ms, 2 warps per sum 208-240 ms)
         SearchArgs b = a;
         b.warps = 16;
-        b.group = 2;
-        b.chunk = 64;
-        return launch_group<16, 2>(b, sms, stream);
+        b.chunk = 8;
+        return launch_w<16, false, 8>(b, sms, stream);
     }
     if (a.group == 2 || a.group == 4) {
         switch (a.warps) {
@@ -958,8 +1014,8 @@ int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
     switch (a.warps) {
     case 4: return launch_map_only<4>(a, sms, stream);
     case 16: return launch_map_only<16>(a, sms, stream);
-    // unset (a work queue, or a chunk given): 8 warps (2^21 job on one box: 236 ms with 8-warp
-    // blocks, 242 ms with 4, 319 ms with 16)
+    // unset (a work queue, or a chunk given): 8 warps (2^21 job on one box with 32-sum chunks:
+    // 220 ms with 8-warp blocks, 221 ms with 4, 219 ms with 16)
     default: return launch_map_only<8>(a, sms, stream);
     }
 }
