@@ -278,7 +278,7 @@ def ours(args, rank, world, dist):
     if rank == 0:
         import numpy as np
         text = ffb.emit((5, LIMIT), full.cpu().numpy().view(np.uint64), lo)
-        want = golden("legs.json")[str(LIMIT)]["sha256"] if LIMIT == 2097152 else None
+        want = golden("legs.json").get(str(LIMIT), {}).get("sha256")
         got = hashlib.sha256(norm(text)).hexdigest()
         if want is not None and got != want:
             raise RuntimeError(f"the job's text differs from the reference leg: sha256 {got}")
