@@ -64,6 +64,11 @@ DEFAULT_TILE = 216 * 1024   # the sieve's shared-memory tile when the caller doe
 # (tests/golden/search_work.json, made by tests/golden/make_search_work.py).
 OP_COST = {"isprime_calls": 6, "splits": 12, "abop_calls": 18, "trial_steps": 10, "divisors": 18}
 
+# DRAM bytes (read + written) per launch of each kernel on the 2^21 job, from one ncu capture
+# of this bench's workload (dram__bytes_read.sum + dram__bytes_write.sum, one pass, full
+# size; the command and the figures are in profiles/launches_ff_sieve_5_2097152.md).
+NCU_TRAFFIC_2_21 = {"sieve_tiles": 0.03235e9 + 22.8528e9, "search_kernel": 452.313e9 + 0.1678e9}
+
 
 def odd_sums(lo, hi):
     return (hi - lo) // 2 + 1 if hi >= lo else 0
@@ -322,10 +327,14 @@ def ours(args, rank, world, dist):
         n_comb, n_wheel = n_comb / world, n_wheel / world
     mark_floor_s = n_comb / peaks["atomsConflictFreePerS"] + n_wheel / peaks["atomsRandomPerS"]
     sieve_kernel_s = sieve_ms / 1e3
+    traffic_src = "ncu capture of this workload on one B200 (profiles/launches_ff_sieve_5_2097152.md)"
+    known = LIMIT == 2097152 and not args.map_bound
     sieve_roof = {
         "kernel": "sieve_tiles", "bound": "hbm", "achieved": sieve_bytes / sieve_kernel_s / 1e9,
         "peak": hbm, "unit": "GB/s", "frac": sieve_bytes / sieve_kernel_s / 1e9 / hbm,
-        "traffic": None, "peak_source": hbm_src, "algorithmic_bytes": sieve_bytes,
+        "traffic": NCU_TRAFFIC_2_21["sieve_tiles"] / world if known else None,
+        "traffic_source": traffic_src if known else None,
+        "peak_source": hbm_src, "algorithmic_bytes": sieve_bytes,
         "marks": n_comb + n_wheel, "marks_per_s": (n_comb + n_wheel) / sieve_kernel_s,
         "marking_floor_ms": 1e3 * mark_floor_s,
         "frac_of_marking_floor": mark_floor_s / sieve_kernel_s,
@@ -339,7 +348,9 @@ def ours(args, rank, world, dist):
     search_roof = {
         "kernel": "search_kernel", "bound": "int_alu", "achieved": ops / (search_ms / 1e3),
         "peak": peaks["intOpsPerS"], "unit": "int ops/s",
-        "frac": ops / (search_ms / 1e3) / peaks["intOpsPerS"], "traffic": None,
+        "frac": ops / (search_ms / 1e3) / peaks["intOpsPerS"],
+        "traffic": NCU_TRAFFIC_2_21["search_kernel"] * (ops / search_ops()[0]) if known else None,
+        "traffic_source": traffic_src if known else None,
         "peak_source": "measured (ffb_measure_peaks: integer multiply-add and ALU chains, "
                        "one IMAD to two ALU operations, whole GPU)",
         "algorithmic_ops": ops, "op_cost": OP_COST, "work_per_job": work,
