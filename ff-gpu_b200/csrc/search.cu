@@ -750,13 +750,14 @@ __device__ __forceinline__ void search_body(const SearchArgs& A)
                 if constexpr (kMR) {
                     if (open) open = settle_mr(st, Q, A, lane, true);
                 } else {
-                    while (open && st.na > 0) {
-                        drain_a(st, Q, A, lane);
-                        if (st.nb >= 32) { drain_b(st, Q, A, lane); open = st.count <= 1; }
-                    }
-                    while (open && st.nb > 0) {
-                        drain_b(st, Q, A, lane);
-                        open = st.count <= 1;
+                    // stage 1 first while queue b has room, then stage 2 (one copy of each)
+                    while (open && (st.na > 0 || st.nb > 0)) {
+                        if (st.na > 0 && st.nb < 32) {
+                            drain_a(st, Q, A, lane);
+                        } else {
+                            drain_b(st, Q, A, lane);
+                            open = st.count <= 1;
+                        }
                     }
                 }
                 if (open && st.count == 1 && lane == 0) write_result<kMR>(A, st.s, sri, st.ta, st.tb);
@@ -902,13 +903,13 @@ __global__ void __launch_bounds__(W * 32, kWarpsPerSm / W) search_kernel_group(c
             }
             if (open) open = run_phase<true, false, G>(st, Q, A, lane, &grp);
             if (open) open = run_phase<false, false, G>(st, Q, A, lane, &grp);
-            while (open && st.na > 0) {
-                drain_a(st, Q, A, lane);
-                if (st.nb >= 32) { drain_b<false, G>(st, Q, A, lane, &grp); open = st.count <= 1; }
-            }
-            while (open && st.nb > 0) {
-                drain_b<false, G>(st, Q, A, lane, &grp);
-                open = st.count <= 1;
+            while (open && (st.na > 0 || st.nb > 0)) {
+                if (st.na > 0 && st.nb < 32) {
+                    drain_a(st, Q, A, lane);
+                } else {
+                    drain_b<false, G>(st, Q, A, lane, &grp);
+                    open = st.count <= 1;
+                }
             }
             group_bar(bar, nthr);
             if (part == 0 && lane == 0 && gs.count == 1)
