@@ -37,6 +37,17 @@ namespace {
 // warps): the search waits on map reads, and more resident warps beat fewer spills.
 constexpr int kWarpsPerSm = FFB_SEARCH_WARPS_PER_SM;
 constexpr int kQueue = 64;       // per-warp queue capacity (entries)
+#ifndef FFB_DRAIN_A
+#define FFB_DRAIN_A 32
+#endif
+#ifndef FFB_DRAIN_B
+#define FFB_DRAIN_B 32
+#endif
+// Queue sizes at which the map-only kernels run stage 1 and stage 2 (at most 32 each, so a
+// queue never passes 63 entries). Full warps win: running stage 2 at 16, 8 or 4 queued items
+// (a sum's rejection found sooner, fewer lanes busy) took the 2^21 search from 199 ms to 244,
+// 304 and 377 ms, and stage 1 at 16 as well to 262 ms.
+constexpr uint32_t kDrainA = FFB_DRAIN_A, kDrainB = FFB_DRAIN_B;
 constexpr int kMaxDiv = 64;      // divisor list of one AllButOne... call (Miller-Rabin variant)
 
 // Stage 2 works in a per-lane scratch of shared memory (no local memory): word j of a lane
@@ -620,9 +631,9 @@ __device__ bool run_phase(SumState& st, WarpQ<kMR>& Q, const SearchArgs& A, int 
                         st.nc = push(Q.c, st.nc, cls == 2, enc(k, o, true), lane);
                     if ((st.na >= 32 || st.nc >= 32) && !settle_mr(st, Q, A, lane, false))
                         return false;
-                } else if (st.na >= 32) {
+                } else if (st.na >= kDrainA) {
                     drain_a(st, Q, A, lane);
-                    if (st.nb >= 32) {
+                    if (st.nb >= kDrainB) {
                         drain_b<kMR, G>(st, Q, A, lane, grp);
                         if (st.count > 1) return false;
                     }
@@ -740,7 +751,7 @@ __device__ __forceinline__ void search_body(const SearchArgs& A)
                 bool open = true;
                 if constexpr (kMR) {
                     if (st.nb >= 32) open = settle_mr(st, Q, A, lane, false);
-                } else if (st.nb >= 32) {
+                } else if (st.nb >= kDrainB) {
                     drain_b(st, Q, A, lane);
                     open = st.count <= 1;
                 }
@@ -897,7 +908,7 @@ __global__ void __launch_bounds__(W * 32, kWarpsPerSm / W) search_kernel_group(c
             // Power2Composite items (reference/segmentedSieve.C:591-605), every G-th to this warp
             st.nb = push(Q.b, 0, ((cmask >> lane) & 1) && lane % G == part, enc(lane, 0, true), lane);
             bool open = true;
-            if (st.nb >= 32) {
+            if (st.nb >= kDrainB) {
                 drain_b<false, G>(st, Q, A, lane, &grp);
                 open = st.count <= 1;
             }
