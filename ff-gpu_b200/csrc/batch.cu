@@ -108,6 +108,8 @@ SearchArgs search_args(const FfbBatch* b, const DeviceState* s)
     a.gcount = nullptr;
     a.tdiv = s->tdiv;
     a.ntdiv = s->ntdiv;
+    a.spf = s->spf;
+    a.spf_limit = s->spf_limit;
     a.sched = b->d_words;
     a.err = b->d_words + 1;
     a.stats = nullptr;

@@ -21,6 +21,28 @@ DeviceState g_states[kMaxDevices];
 std::mutex g_state_mu;
 unsigned g_sched_next[kMaxDevices];
 
+// The terms the search factors are below its largest sum, at most 2^25 + 1.
+constexpr uint32_t kSpfLimit = (1u << 25) + 2;
+
+// spf[i] for the odd n = 2i + 1: the index in tdiv of n's smallest prime factor, 0xFFFF for
+// 1 and the primes (a composite below kSpfLimit has a factor below 5,793, inside the table).
+__global__ void build_spf(const TDiv* tdiv, uint32_t ntdiv, uint16_t* spf, uint32_t nodd)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nodd; i += gridDim.x * blockDim.x) {
+        const uint32_t n = 2 * i + 1;
+        uint16_t r = 0xFFFF;
+        for (uint32_t k = 0; k < ntdiv; ++k) {
+            const TDiv t = tdiv[k];
+            if ((uint64_t)t.p * t.p > n) break;
+            if (n * t.inv <= t.lim) {
+                r = (uint16_t)k;
+                break;
+            }
+        }
+        spf[i] = r;
+    }
+}
+
 bool device_visible(int dev)
 {
     int n = 0;
@@ -71,6 +93,21 @@ DeviceState* device_state(int dev)
         cudaGetLastError();
         return nullptr;
     }
+    // the smallest-prime-factor table, made once on the device (a few milliseconds)
+    const uint32_t nodd = kSpfLimit / 2;
+    uint16_t* spf = nullptr;
+    if (cudaMalloc(&spf, sizeof(uint16_t) * nodd) != cudaSuccess) {
+        std::fprintf(stderr, "ffb: device %d state allocation failed\n", dev);
+        cudaGetLastError();
+        return nullptr;
+    }
+    build_spf<<<prop.multiProcessorCount * 8, 256>>>(dt, npr, spf, nodd);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+        std::fprintf(stderr, "ffb: device %d factor table failed\n", dev);
+        return nullptr;
+    }
+    s.spf = spf;
+    s.spf_limit = kSpfLimit;
     s.sms = prop.multiProcessorCount;
     s.tdiv = dt;
     s.ntdiv = npr;
@@ -119,6 +156,8 @@ int run_search(int dev, const uint8_t* d_map, uint64_t bound, uint32_t lo, uint3
     a.gcount = gcount;
     a.tdiv = s->tdiv;
     a.ntdiv = s->ntdiv;
+    a.spf = s->spf;
+    a.spf_limit = s->spf_limit;
     a.sched = sched_slot(s);
     a.err = err_word(s);
     a.stats = stats_words(s);

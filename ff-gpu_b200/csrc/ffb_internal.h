@@ -37,6 +37,10 @@ struct SearchArgs {
     uint32_t chunk = 32;    // sums a warp takes per pull of the work counter: 16, 32 or 64
                             // (one warp per sum), 32 * group with group > 1
     uint32_t group = 1;     // warps per sum: 1, or 2 / 4 (map-only variant)
+    // smallest prime factor of each odd n < spf_limit: spf[n >> 1] is its index in tdiv, or
+    // 0xFFFF when n is 1 or prime (null: factorisations by trial division alone)
+    const uint16_t* spf = nullptr;
+    uint32_t spf_limit = 0;
 };
 
 // Packed per-sum record written by the search: 0 = no solution line, else
@@ -54,6 +58,8 @@ struct DeviceState {
     TDiv* tdiv = nullptr;
     uint32_t ntdiv = 0;
     uint32_t* words = nullptr;  // [0..63] scheduler counters, [64] error flags
+    uint16_t* spf = nullptr;    // smallest-prime-factor table (SearchArgs::spf), 32 MB
+    uint32_t spf_limit = 0;
 };
 DeviceState* device_state(int device);  // nullptr (and a stderr line) on failure
 

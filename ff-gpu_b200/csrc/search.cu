@@ -124,14 +124,27 @@ __device__ __forceinline__ int pair_class(const SearchArgs& A, uint64_t i)
     return above_map_class(n, A.err);
 }
 
-// Ascending prime factorisation of an odd x < 2^32 by the exact-division table, with the
-// cofactor's primality read from the bitmap after every factor found: put(q, e) receives
-// the prime powers in ascending order.
+// Ascending prime factorisation of an odd x < 2^32: by the smallest-prime-factor table when
+// x lies inside it, else by the exact-division table with the cofactor's primality read from
+// the bitmap after every factor found. put(q, e) receives the prime powers in ascending order.
 template <bool kMR, class Put>
 __device__ __forceinline__ void factor_odd(uint32_t x, const SearchArgs& A, Put&& put)
 {
     uint32_t n = x;
     if (n <= 1) return;
+    if (n < A.spf_limit) {
+        // the smallest-prime-factor table: one lookup per distinct prime factor, and the
+        // cofactor's primality from the same table
+        for (;;) {
+            const uint32_t idx = __ldg(A.spf + (n >> 1));
+            if (idx == 0xFFFFu) { put(n, 1u); return; }
+            const TDiv t = A.tdiv[idx];
+            uint32_t ex = 0, y = n * t.inv;
+            do { n = y; ++ex; y = n * t.inv; } while (y <= t.lim);
+            put(t.p, ex);
+            if (n == 1) return;
+        }
+    }
     if (isp<kMR>(A, n)) { put(n, 1u); return; }
     for (uint32_t i = 0; i < A.ntdiv; ++i) {
         const TDiv t = A.tdiv[i];
@@ -668,7 +681,7 @@ __device__ void write_result(const SearchArgs& A, uint32_t s, uint32_t ri, uint3
 template <int W, bool kMR, int K>
 __device__ __forceinline__ void search_body(const SearchArgs& A)
 {
-    static_assert(K == 8 || K == 16 || K == 32 || K == 64, "sums per chunk");
+    static_assert(K == 16 || K == 32 || K == 64, "sums per chunk");
     __shared__ WarpQ<kMR> queues[W];
     const int lane = threadIdx.x & 31;
     WarpQ<kMR>& Q = queues[threadIdx.x >> 5];
@@ -1001,13 +1014,14 @@ int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
         return -1;
     }
     if (a.warps == 0 && a.group == 1 && a.chunk == 32 && a.nseg == 0 && !mr) {
-        // unset shape on one range over a map covering every probe: 16 warps a block, one per
-        // sum, 8-sum chunks (2^21 job on one box: 202.5 ms; 16-sum chunks 203-206 ms, 4 or 8
-        // warps the same, 32-sum chunks 213 ms, 2 warps per sum 208-240 ms)
+        // unset shape on one range over a map covering every probe: 16 warps a block, 2 per
+        // sum, 64-sum chunks (2^21 job on one box: 187.5 ms; 4 per sum 219 ms, one warp per
+        // sum 216-256 ms)
         SearchArgs b = a;
         b.warps = 16;
-        b.chunk = 8;
-        return launch_w<16, false, 8>(b, sms, stream);
+        b.group = 2;
+        b.chunk = 64;
+        return launch_group<16, 2>(b, sms, stream);
     }
     if (a.group == 2 || a.group == 4) {
         switch (a.warps) {
@@ -1027,7 +1041,7 @@ int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
     case 4: return launch_map_only<4>(a, sms, stream);
     case 16: return launch_map_only<16>(a, sms, stream);
     // unset (a work queue, or a chunk given): 8 warps (2^21 job on one box with 32-sum chunks:
-    // 220 ms with 8-warp blocks, 221 ms with 4, 219 ms with 16)
+    // 225-228 ms with 8-warp blocks, 226-229 ms with 4, 228-234 ms with 16)
     default: return launch_map_only<8>(a, sms, stream);
     }
 }

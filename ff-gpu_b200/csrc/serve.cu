@@ -304,6 +304,8 @@ int enqueue(FfbServer* S, Slot& sl, uint32_t top)
     a.gcount = nullptr;
     a.tdiv = S->ds->tdiv;
     a.ntdiv = S->ds->ntdiv;
+    a.spf = S->ds->spf;
+    a.spf_limit = S->ds->spf_limit;
     a.sched = reinterpret_cast<uint32_t*>(sl.d_q);
     a.err = reinterpret_cast<uint32_t*>(sl.d_q) + 1;
     a.stats = S->d_stats;
