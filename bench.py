@@ -67,7 +67,7 @@ OP_COST = {"isprime_calls": 6, "splits": 12, "abop_calls": 18, "trial_steps": 10
 # DRAM bytes (read + written) per launch of each kernel on the 2^21 job, from one ncu capture
 # of this bench's workload (dram__bytes_read.sum + dram__bytes_write.sum, one pass, full
 # size; the command and the figures are in profiles/launches_ff_sieve_5_2097152.md).
-NCU_TRAFFIC_2_21 = {"sieve_tiles": 0.03235e9 + 22.8528e9, "search_kernel": 452.313e9 + 0.1678e9}
+NCU_TRAFFIC_2_21 = {"sieve_tiles": 0.03426e9 + 22.8534e9, "search_kernel": 463.360e9 + 2.707e9}
 
 
 def odd_sums(lo, hi):
