@@ -33,7 +33,7 @@ struct SearchArgs {
                             // chunk}, largest sums first (or null: the single range lo..hi)
     uint32_t nseg = 0;      // intervals in seg (0: single range)
     uint32_t nchunks = 0;   // chunks of `chunk` sums over all intervals
-    uint32_t warps = 0;     // warps per block: 4, 8 or 16 (0: 16 map-only, 8 Miller-Rabin)
+    uint32_t warps = 0;     // warps per block: 4, 8 or 16 (0: 16 map-only, 4 Miller-Rabin)
     uint32_t chunk = 32;    // sums a warp takes per pull of the work counter: 16, 32 or 64
                             // (one warp per sum), 32 * group with group > 1
     uint32_t group = 1;     // warps per sum: 1, or 2 / 4 (map-only variant)

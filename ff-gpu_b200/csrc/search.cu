@@ -1032,9 +1032,12 @@ int launch_search(const SearchArgs& a, int sms, cudaStream_t stream)
     }
     if (mr) {
         switch (a.warps) {
-        case 4: return launch_w<4, true, 32>(a, sms, stream);
+        // unset: 4 warps (the served mode's first 1,000 seed-1 requests: 914k sums/s with
+        // 4-warp blocks, 874k with 16, 843k with 8; 2^21 sums against the served map: 441,
+        // 430 and 494 ms)
+        case 8: return launch_w<8, true, 32>(a, sms, stream);
         case 16: return launch_w<16, true, 32>(a, sms, stream);
-        default: return launch_w<8, true, 32>(a, sms, stream);   // unset: 8 (the served mode's best)
+        default: return launch_w<4, true, 32>(a, sms, stream);
         }
     }
     switch (a.warps) {
