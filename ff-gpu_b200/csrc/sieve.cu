@@ -220,10 +220,19 @@ __global__ void __launch_bounds__(kSieveThreads) sieve_tiles(const TileArgs A)
             for (uint32_t b = f + 32u * p32 * lane; ; b += step) {
                 if (!__any_sync(0xFFFFFFFFu, b < rl)) break;
                 uint32_t x = b;
+                if (__all_sync(0xFFFFFFFFu, b + 31u * p32 < rl)) {
+                    // every lane's 32 marks lie in the tile: no bound test per mark
 #pragma unroll 8
-                for (int r = 0; r < 32; ++r) {
-                    if (x < rl) atomicAnd(&tile[x >> 5], clear_mask(x));
-                    x += p32;
+                    for (int r = 0; r < 32; ++r) {
+                        atomicAnd(&tile[x >> 5], clear_mask(x));
+                        x += p32;
+                    }
+                } else {
+#pragma unroll 8
+                    for (int r = 0; r < 32; ++r) {
+                        if (x < rl) atomicAnd(&tile[x >> 5], clear_mask(x));
+                        x += p32;
+                    }
                 }
             }
         }
