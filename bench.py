@@ -166,11 +166,11 @@ def odd_primes_upto(n):
 
 def sieve_marks(mpv, tile_bytes):
     """Shared-memory marks sieve_tiles makes for the map of values 0..mpv: the comb primes
-    (83 <= p <= tile bits / 2048) mark every odd multiple from p^2, the larger primes the
-    multiples p*k, k >= p, with k prime to 30 (the patterns cover 3..79)."""
+    (47 <= p <= tile bits / 2048) mark every odd multiple from p^2, the larger primes the
+    multiples p*k, k >= p, with k prime to 30 (the patterns cover 3..43)."""
     import numpy as np
     p = odd_primes_upto(math.isqrt(mpv))
-    p = p[p >= 83]
+    p = p[p >= 47]
     pcomb = tile_bytes * 8 // 2048
     comb = p[p <= pcomb]
     wheel = p[p > pcomb]

@@ -16,19 +16,20 @@
 // kernel and every other entry through sieve_generic.
 //
 // sieve_tiles (persistent grid over shared-memory tiles):
-//   1. A tile starts as the AND of eight pre-computed patterns (the odd numbers free of
-//      3..13, of 17,19,23, of 29,31,37 and of the pairs 41*43 .. 73*79), read with funnel
-//      shifts at 32-bit phases advanced incrementally per word: no prime up to 79 is marked.
-//   2. Small primes (p <= tile bits / 1024, at least 32 marks per lane): the "comb". The warp
+//   1. A tile starts as the AND of four pre-computed patterns (the odd numbers free of
+//      3..13, of 17,19,23, of 29,31,37 and of 41*43), read with funnel shifts at 32-bit
+//      phases advanced incrementally per word: no prime up to 43 is marked.
+//   2. Small primes (p <= tile bits / 2048, at least 64 marks per lane): the "comb". The warp
 //      takes one prime; at each step its 32 lanes mark the multiples f + p*(r + 32*lane + 1024*t)
 //      for the same r, which lie 32p bits = p words apart: the same bit of 32 words whose
 //      banks (word + p*lane) mod 32 are all different because p is odd. Every shared-memory
-//      atomic of the comb is free of bank conflicts.
+//      atomic of the comb is free of bank conflicts; a round whose 32 marks per lane all lie
+//      in the tile runs with no bound test.
 //   3. Larger primes: one thread per prime, stepping over the multiples p*k with k prime to
 //      30 only (the mod-30 wheel: steps of 3p, 2p, p, 2p, p, 2p, 3p, p bits). The multiples
 //      with k divisible by 3 or 5 are multiples of 3 or 5, already cleared by the patterns,
 //      so 7 of every 15 odd multiples are never marked. (Without the patterns, a caller list
-//      that lacks 3..79, every odd multiple is stepped.)
+//      that lacks 3..43, every odd multiple is stepped.)
 //   Warps take comb primes (smallest first) and groups of 32 larger primes from per-tile
 //   shared counters, so a warp that finishes early takes more work.
 //   4. The tile is converted to the reference bit order (brev + byte swap) and written to
@@ -45,7 +46,7 @@ namespace ffb {
 
 // Device-side description of the marking list (written by list_primes or uploaded):
 // primes [0, n) ascending; [ibeg, icomb) are comb primes, [icomb, n) one thread each
-// (ibeg skips the pattern primes 3..79 when the patterns are applied).
+// (ibeg skips the pattern primes 3..43 when the patterns are applied).
 struct SieveListHeader {
     uint32_t n, ibeg, icomb, pad;
 };
@@ -59,30 +60,27 @@ constexpr uint32_t kListSegWords = 8192;   // list_primes segment: 262,144 odd v
 // Pre-sieve patterns: bit j (LSB-first) of pattern g is 1 iff the odd number 2j+1 has no
 // factor among the primes of group g; each pattern repeats with the product of its primes (in
 // odd numbers) and is stored with one extra period word so any 32-bit window can be read
-// without wrapping. Groups 0..2 cover 3..37 (list_primes uses those three), groups 3..7 the
-// pairs 41*43, 47*53, 59*61, 67*71, 73*79: a pattern costs a few instructions per 32-bit word,
-// far less than the shared-memory atomics the marks of those primes would cost.
-constexpr int kGroups = 8;
+// without wrapping. Groups 0..2 cover 3..37 (list_primes uses those three), group 3 the pair
+// 41*43. A pattern costs some six instructions per 32-bit word; the comb marks of a pair of
+// primes near 50 cost about as much, and above that less (the 2^21 map: patterns for 3..43
+// 98.4 ms, for 3..61 99.3 ms, for 3..79 101.2 ms).
+constexpr int kGroups = 4;
 constexpr uint32_t kPeriod0 = 3 * 5 * 7 * 11 * 13;   // 15015
 constexpr uint32_t kPeriod1 = 17 * 19 * 23;          // 7429
 constexpr uint32_t kPeriod2 = 29 * 31 * 37;          // 33263
-constexpr uint32_t kPeriod3 = 41 * 43, kPeriod4 = 47 * 53, kPeriod5 = 59 * 61,
-                   kPeriod6 = 67 * 71, kPeriod7 = 73 * 79;
+constexpr uint32_t kPeriod3 = 41 * 43;               // 1763
 __host__ __device__ constexpr uint32_t words_of(uint32_t period) { return (period + 63) / 32 + 1; }
 constexpr uint32_t kWords0 = words_of(kPeriod0);
 constexpr uint32_t kWords1 = words_of(kPeriod1);
 constexpr uint32_t kWords2 = words_of(kPeriod2);
-constexpr uint32_t kWheelWords = kWords0 + kWords1 + kWords2 + words_of(kPeriod3) +
-                                 words_of(kPeriod4) + words_of(kPeriod5) + words_of(kPeriod6) +
-                                 words_of(kPeriod7);
-constexpr int kWheelPrimes = 21;                     // 3 .. 79
-constexpr uint32_t kLastPatternPrime = 79;
+constexpr uint32_t kWheelWords = kWords0 + kWords1 + kWords2 + words_of(kPeriod3);
+constexpr int kWheelPrimes = 13;                     // 3 .. 43
+constexpr uint32_t kLastPatternPrime = 43;
 __device__ uint32_t g_wheel[kWheelWords];
 
 __host__ __device__ constexpr uint32_t group_period(int g)
 {
-    return g == 0 ? kPeriod0 : g == 1 ? kPeriod1 : g == 2 ? kPeriod2 : g == 3 ? kPeriod3
-         : g == 4 ? kPeriod4 : g == 5 ? kPeriod5 : g == 6 ? kPeriod6 : kPeriod7;
+    return g == 0 ? kPeriod0 : g == 1 ? kPeriod1 : g == 2 ? kPeriod2 : kPeriod3;
 }
 __host__ __device__ constexpr uint32_t group_offset(int g)
 {
@@ -104,7 +102,7 @@ struct TileArgs {
     const uint32_t* primes; // marking list (device)
     const uint64_t* mu;     // floor((2^64-1) / p) per prime
     const SieveListHeader* hdr;
-    int wheel;              // the patterns are applied (the list holds 3..79)
+    int wheel;              // the patterns are applied (the list holds 3..43)
     int clear_one;          // clear the bit of the value 1 (seg_lo == 0)
     uint32_t tile_words;
     uint64_t ntiles;
@@ -180,17 +178,13 @@ __global__ void __launch_bounds__(kSieveThreads) sieve_tiles(const TileArgs A)
             const uint64_t j = j0 + m0 + 32ull * threadIdx.x;
             constexpr uint32_t adv = 32u * kSieveThreads;
             uint32_t ph0 = (uint32_t)(j % kPeriod0), ph1 = (uint32_t)(j % kPeriod1),
-                     ph2 = (uint32_t)(j % kPeriod2), ph3 = (uint32_t)(j % kPeriod3),
-                     ph4 = (uint32_t)(j % kPeriod4), ph5 = (uint32_t)(j % kPeriod5),
-                     ph6 = (uint32_t)(j % kPeriod6), ph7 = (uint32_t)(j % kPeriod7);
+                     ph2 = (uint32_t)(j % kPeriod2), ph3 = (uint32_t)(j % kPeriod3);
             for (uint32_t w = threadIdx.x; w < words; w += kSieveThreads) {
                 const uint64_t gm = m0 + 32ull * w;
                 uint32_t x = 0xFFFFFFFFu;
                 if (A.wheel) {
                     x = pattern_word<0, adv>(wheel, ph0) & pattern_word<1, adv>(wheel, ph1) &
-                        pattern_word<2, adv>(wheel, ph2) & pattern_word<3, adv>(wheel, ph3) &
-                        pattern_word<4, adv>(wheel, ph4) & pattern_word<5, adv>(wheel, ph5) &
-                        pattern_word<6, adv>(wheel, ph6) & pattern_word<7, adv>(wheel, ph7);
+                        pattern_word<2, adv>(wheel, ph2) & pattern_word<3, adv>(wheel, ph3);
                 }
                 if (gm + 32 > A.nbits) {  // bits of values >= seg_hi stay set
                     const uint64_t keep = A.nbits > gm ? A.nbits - gm : 0;
@@ -269,8 +263,7 @@ __global__ void __launch_bounds__(kSieveThreads) sieve_tiles(const TileArgs A)
         __syncthreads();
         // ---- the pattern primes themselves and the value 1 ----
         if (threadIdx.x == 0 && A.base_odd <= kLastPatternPrime) {
-            const uint32_t wp[kWheelPrimes] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37,
-                                               41, 43, 47, 53, 59, 61, 67, 71, 73, 79};
+            const uint32_t wp[kWheelPrimes] = {3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43};
             if (A.wheel)
                 for (int q = 0; q < kWheelPrimes; ++q) {
                     if (wp[q] < A.base_odd) continue;
@@ -479,8 +472,7 @@ int upload_wheel()
     FFB_CUDA(cudaGetDevice(&dev));
     if (done_dev == dev) return 0;
     std::vector<uint32_t> w(kWheelWords, 0);
-    const uint32_t group[kGroups][5] = {{3, 5, 7, 11, 13}, {17, 19, 23}, {29, 31, 37}, {41, 43},
-                                        {47, 53},          {59, 61},     {67, 71},     {73, 79}};
+    const uint32_t group[kGroups][5] = {{3, 5, 7, 11, 13}, {17, 19, 23}, {29, 31, 37}, {41, 43}};
     for (int g = 0; g < kGroups; ++g) {
         const uint32_t off = group_offset(g), period = group_period(g);
         for (uint32_t jj = 0; jj < words_of(period) * 32; ++jj) {
@@ -598,7 +590,7 @@ int analyse(const SieveArgs& a, int sms, SieveHost& H)
         // primes of the standard prefix with p*p < seg_hi mark something
         uint32_t iend = 0;
         while (iend < std_n && (uint64_t)h[off + iend] * h[off + iend] < a.seg_hi) ++iend;
-        wheel = std_n >= kWheelPrimes;  // the patterns need 3..79 in the list
+        wheel = std_n >= kWheelPrimes;  // the patterns need 3..43 in the list
         H.list.assign(h + off, h + off + iend);
         H.mu.resize(iend);
         for (uint32_t i = 0; i < iend; ++i) H.mu[i] = ~0ull / h[off + i];   // Barrett constants
