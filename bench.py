@@ -316,7 +316,8 @@ def ours(args, rank, world, dist):
         lib.ffb_context_destroy(ctx)
         e2e = {"value": job_sums / statistics.mean(times), "unit": UNIT,
                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 8 * job_sums,
-               "text_bytes_per_step": text_len, "ms_per_step": 1e3 * statistics.mean(times)}
+               "text_bytes_per_step": text_len, "ms_per_step": 1e3 * statistics.mean(times),
+               "step_ms": [round(1e3 * t, 2) for t in times]}
 
     hbm, hbm_src = hbm_peak()
     # sieve: HBM bytes written once, and the shared-memory marks against the measured atomic
