@@ -344,7 +344,7 @@ int ffb_shrink_budget(uint64_t freeBytes, double fraction, uint64_t capBytes,
 /* while others run. The device keeps one prime map resident (sieved at creation up to */
 /* the bound the first requests need, grown to the largest admitted limit, never past  */
 /* the budget's backing bytes; Miller-Rabin answers probes above it, so every answer is */
-/* the same as with the reference's own map), the trial-division table and, per launch */
+/* the same as with the reference's own map), the factor tables and, per launch       */
 /* slot, record and work-queue buffers carved from the budget's scratch bytes.          */
 /* Continuous batching: whenever a launch slot is free, the scheduler fills one search  */
 /* launch with a slice of every waiting request (oldest first, each request's sums in   */
