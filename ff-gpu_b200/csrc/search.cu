@@ -1,24 +1,26 @@
 // search.cu -- the per-sum Freudenthal search (reference/segmentedSieve.C:419-639, 800-823).
 //
 // Parallel structure (sm_100a, SIMT integer code):
-//   * A persistent grid; each warp pulls chunks of 32 consecutive odd sums from a device
-//     counter, largest sums first (their cost grows with the sum, so big ones start early).
-//   * Lane-parallel over the 32 sums: Sammy's first statement (the RunIt filter) and the
-//     Power2Prime phase. A sum still open after that (at most one valid split so far) is a
-//     "survivor".
+//   * A persistent grid; each warp (or group of warps) pulls chunks of consecutive odd sums
+//     from a device counter, largest sums first (their cost grows with the sum, so big ones
+//     start early).
+//   * Lane-parallel over up to 32 sums per warp: Sammy's first statement (the RunIt filter)
+//     and the Power2Prime phase. A sum still open after that (at most one valid split so
+//     far) is a "survivor".
 //   * Warp-cooperative per survivor: lanes enumerate the Power2Odd / Power2Even splits
 //     (k, o) in parallel. The verdict of the reference depends only on WHETHER exactly one
 //     split is valid (and then on that split), not on the order the splits are visited, so
 //     the order is free and the warp stops as soon as two valid splits are seen.
 //   * Rare, expensive work is deferred through per-warp shared-memory queues so lanes stay
 //     converged: stage 0 (every split) runs the divisibility filters and the pair probe
-//     o + b*2^k - 2, whose values are small (bitmap prefix, cache resident); stage 1 (about
-//     one split in eight) probes 2^k + o*b - 2, a random HBM sector; stage 2 (about one in
-//     a hundred) runs AllButOne... on the split's product.
-//   * AllButOne... is evaluated from the factorisations of o and b (both below the sum)
-//     instead of the reference's trial-division walk over all primes: the pairs that walk
-//     tests are exactly those of the odd divisors up to the square-root limit and their
-//     2^k multiples, which an odometer over the exponents enumerates with no divisor list.
+//     o + b*2^k - 2; stage 1 (about one split in seven) probes 2^k + o*b - 2; stage 2 (about
+//     one split in sixty) runs AllButOne... on the split's product. Both probes read random
+//     sectors of the map for all but the smallest k.
+//   * AllButOne... is evaluated from the factorisations of o and b (both below the sum, read
+//     from a smallest-prime-factor table) instead of the reference's trial-division walk over
+//     all primes: the pairs that walk tests are exactly those of the odd divisors up to the
+//     square-root limit and their 2^k multiples, which an odometer over the exponents
+//     enumerates with no divisor list.
 //   * Launch shapes (the candidates the batch's autotuner times): 4, 8 or 16 warps a block;
 //     16, 32 or 64 sums per pull of the work counter (a compile-time parameter, so the
 //     one-warp-per-sum kernel carries no extra loop); or 2 or 4 warps sharing one sum
